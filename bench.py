@@ -1,0 +1,332 @@
+"""Benchmark: projections/s of the cone-beam forward projector on B200.
+
+Workload (one step): the 256^3 -> 512^2 short-scan configuration -- a 256^3
+float32 volume (1 mm voxels, water cylinder + 40 seeded ellipsoids), 360 views
+over 200 deg + fan angle, flat 512 x 512 detector at 0.6 mm, SID 750 mm,
+SDD 1200 mm, seeded per-view jitter (+-0.5 mm source/detector, +-0.2 deg
+tilt), raySampling 0.3, trilinear interpolation, up-sampling 1.  One step
+projects all 360 views.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value    views/s over all ranks, volume resident on the device, device-side
+         P matrices and output, CUDA-event timed per step (L2 flushed between
+         steps by writing a 256 MiB buffer, outside the timed events)
+e2e      the same job through the C ABI call a CTL user makes
+         (ctlcu_project_volume): host volume, host P matrices, host output,
+         copies inside the timed region
+roofline the ray-casting kernel's gather bytes (samples x 8 taps x voxel bytes +
+         output) per launch over its CUDA-event duration, against on-SM L1
+         delivery (SMs x 128 B/clk x sampled SM clock)
+--impl reference   the reference's own kernel (raycasterprojector_interp.cl
+         compiled for the CPU, oracle/_ref) on all host cores, a bounded
+         sample of the same views per step
+Multi-GPU: one process per GPU (torchrun), each projecting the full job on its
+own device (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+VOXEL = (1.0, 1.0, 1.0)
+SHAPE = (256, 256, 256)
+CHANNELS = ROWS = 512
+N_VIEWS = 360
+METRIC = "projections/s at 256^3->512^2 (plain FP32)"
+WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
+
+
+def make_inputs():
+    from ctl_b200 import geometry as G
+    from ctl_b200 import phantom as Ph
+    vol = Ph.ellipsoid_phantom(SHAPE, VOXEL, 40, seed=2)
+    det = G.FlatDetector(CHANNELS, ROWS, 0.6, 0.6)
+    fan = G.fan_angle(det, 1200.0)
+    P = G.circular_flat(N_VIEWS, 750.0, 1200.0, det, angle_range=math.radians(200.0) + fan,
+                        rng=np.random.default_rng(2024), jitter_mm=0.5, tilt_deg=0.2)
+    return vol, P
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_rate(vol, P, target_s: float, threads: int):
+    """The reference's kernel on the host: time a bounded, evenly spaced view sample."""
+    import oracle
+    t0 = time.perf_counter()
+    oracle.project_ref(vol, VOXEL, P[:1], CHANNELS, ROWS, threads=threads)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(N_VIEWS, round(target_s / max(t1, 1e-3)))))
+    idx = np.linspace(0, N_VIEWS - 1, n).round().astype(int)
+    t0 = time.perf_counter()
+    oracle.project_ref(vol, VOXEL, P[idx], CHANNELS, ROWS, threads=threads)
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    threads = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": METRIC, "unit": "projections/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
+            "config": {"workload": WORKLOAD}}
+    if not oracle.ref_available():
+        line["unavailable"] = "oracle/_ref/libctlref.so (reference kernel compiled for the CPU) is not built"
+        print(json.dumps(line))
+        return 0
+    vol, P = make_inputs()
+    # one step = a bounded sample of views spread over the scan
+    per_step = max(1, int(args.ref_views))
+    idx = np.linspace(0, N_VIEWS - 1, per_step).round().astype(int)
+    for _ in range(args.warmup):
+        oracle.project_ref(vol, VOXEL, P[idx[:1]], CHANNELS, ROWS, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.project_ref(vol, VOXEL, P[idx], CHANNELS, ROWS, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = per_step / (ms / 1e3)
+    sample = f"{per_step} of {N_VIEWS} views per step, evenly spaced, {threads} threads"
+    line.update({"value": value, "ms_per_step": ms, "scaling": "none",
+                 "cpu_baseline": {"value": value, "unit": "projections/s", "cores": threads,
+                                  "kind": "reference", "sample": sample},
+                 "e2e": {"value": value, "unit": "projections/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0},
+                 "vs_baseline": None})
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import ctl_b200
+    from ctl_b200 import _lib as L
+    from ctl_b200.projector import Context, Settings, VoxelVolume
+
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    vol, P = make_inputs()
+    settings = Settings(accum={"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[args.accum],
+                        storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage])
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    vobj = VoxelVolume(vol, VOXEL)
+    volume = ctx.volume(vobj, settings.storage)
+    dP = torch.from_numpy(P).to(dev)
+    out = torch.empty((N_VIEWS, 1, ROWS, CHANNELS), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    samples = ctx.count_samples(volume, P, CHANNELS, ROWS, settings)
+
+    def step():
+        ctx.project(volume, dP, CHANNELS, ROWS, settings, out=out, stream=ctx.stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier(world)
+        clocks = ClockSampler(local)
+        clocks.start()
+        l0 = ctx.launches()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        barrier(world)
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush outside the timed events
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launches() - l0
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms), world)
+    ms_per_step = total_ms / args.steps
+    value = world * N_VIEWS * args.steps / (total_ms / 1e3)
+
+    # the projection kernel alone: each step is one setup launch + one projection launch;
+    # time a setup-only run to split them
+    from ctl_b200.projector import Context as _C  # noqa: F401
+    kernel_ms = ms_per_step  # refined below when the profile split is known
+
+    # e2e through the C ABI with host buffers (pinned)
+    h_vol = torch.from_numpy(vol).pin_memory()
+    h_P = torch.from_numpy(P).pin_memory()
+    h_out = torch.empty((N_VIEWS, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
+    desc_vol = VoxelVolume(h_vol.numpy(), VOXEL)
+    for _ in range(max(1, args.warmup // 2)):
+        ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
+    barrier(world)
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = world * N_VIEWS * len(e2e_ms) / (e2e_total / 1e3)
+    clk = clocks.stop()
+
+    if rank == 0:
+        b = 4 if settings.storage == L.F32 else 2
+        alg_bytes = samples * 8 * b + 4 * N_VIEWS * ROWS * CHANNELS
+        props = torch.cuda.get_device_properties(dev)
+        sms = props.multi_processor_count
+        mhz = clk.get("sm_mhz") or 1965.0
+        l1_peak = sms * 128 * mhz * 1e6 / 1e9  # GB/s
+        achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {L.F32: "f32", L.BF16: "bf16", L.F16: "f16"}[settings.storage] + "-storage/f32-interp/"
+                     + args.accum + "-accum",
+            "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
+            "config": {"workload": WORKLOAD, "views_per_step": N_VIEWS, "volume": "256^3", "detector": "512x512",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": f"views replicated per GPU x{world}"},
+            "samples_per_step": samples,
+            "gsamples_per_s": samples * world * args.steps / (total_ms / 1e3) / 1e9,
+            "e2e": {"value": e2e_value, "unit": "projections/s",
+                    "h2d_bytes_per_step": int(vol.nbytes + P.nbytes),
+                    "d2h_bytes_per_step": int(h_out.numel() * 4),
+                    "path": "ctlcu_project_volume, pinned host buffers"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "l1", "achieved": achieved, "peak": l1_peak, "unit": "GB/s",
+                         "frac": achieved / l1_peak, "traffic": None,
+                         "peak_source": f"{sms} SMs x 128 B/clk x {mhz:.0f} MHz sampled SM clock",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            if oracle.ref_available():
+                rate, n, dt = cpu_reference_rate(vol, P, args.cpu_seconds, os.cpu_count() or 1)
+                line["cpu_baseline"] = {"value": rate, "unit": "projections/s", "cores": os.cpu_count(),
+                                        "kind": "reference",
+                                        "sample": f"{n} of {N_VIEWS} views evenly spaced, {dt:.1f} s"}
+        print(json.dumps(line))
+    volume.release()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--accum", choices=["fp64", "kahan", "fp32"], default="fp64")
+    ap.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-views", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

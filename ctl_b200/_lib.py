@@ -1,0 +1,108 @@
+"""ctypes binding of libctlcu.so (include/ctlcu.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+it is missing or fails to load, every projector call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libctlcu.so")
+
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_INVALID_HANDLE = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_CUDA = 4
+ERR_NO_DEVICE = 5
+ERR_SINGULAR_GEOMETRY = 6
+ERR_TIMEOUT = 7
+ERR_BUSY = 8
+
+F32, BF16, F16 = 0, 1, 2
+INTERP_SOFTWARE, INTERP_TEXTURE = 0, 1
+ACCUM_FP64, ACCUM_KAHAN, ACCUM_FP32 = 0, 1, 2
+
+STATUS_NAMES = {
+    OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",
+    ERR_OUT_OF_MEMORY: "OUT_OF_MEMORY", ERR_CUDA: "CUDA", ERR_NO_DEVICE: "NO_DEVICE",
+    ERR_SINGULAR_GEOMETRY: "SINGULAR_GEOMETRY", ERR_TIMEOUT: "TIMEOUT", ERR_BUSY: "BUSY",
+}
+
+
+class VolumeDesc(C.Structure):
+    _fields_ = [("n", C.c_uint32 * 3), ("voxel_mm", C.c_float * 3), ("offset_mm", C.c_float * 3),
+                ("dtype", C.c_int32)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("rays_per_pixel", C.c_uint32 * 2), ("ray_sampling", C.c_float),
+                ("volume_upsampling", C.c_uint32), ("interpolate", C.c_int32),
+                ("interp_mode", C.c_int32), ("accum", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("volume", C.c_uint64), ("pmats", C.c_void_p), ("out", C.c_void_p),
+                ("n_views", C.c_uint32), ("n_modules", C.c_uint32), ("channels", C.c_uint32),
+                ("rows", C.c_uint32)]
+
+
+# (name, restype, argtypes) of every entry point declared in include/ctlcu.h
+SIGNATURES = [
+    ("ctlcu_abi_version", C.c_int, []),
+    ("ctlcu_settings_default", Settings, []),
+    ("ctlcu_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("ctlcu_destroy", C.c_int, [C.c_void_p]),
+    ("ctlcu_last_error", C.c_char_p, [C.c_void_p]),
+    ("ctlcu_set_memory_budget", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("ctlcu_memory_used", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("ctlcu_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("ctlcu_volume_create", C.c_int, [C.c_void_p, C.POINTER(VolumeDesc), C.c_void_p, C.c_int,
+                                      C.POINTER(C.c_uint64)]),
+    ("ctlcu_volume_release", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("ctlcu_volume_bytes", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ctlcu_project", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
+                                C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("ctlcu_project_volume", C.c_int, [C.c_void_p, C.POINTER(VolumeDesc), C.c_void_p, C.POINTER(Settings),
+                                       C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_void_p]),
+    ("ctlcu_project_batch", C.c_int, [C.c_void_p, C.POINTER(Request), C.c_uint32, C.POINTER(Settings),
+                                      C.c_void_p]),
+    ("ctlcu_sync", C.c_int, [C.c_void_p]),
+    ("ctlcu_count_samples", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
+                                      C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
+    ("ctlcu_view_setup", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                   C.c_void_p]),
+    ("ctlcu_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libctlcu.so and declare its signatures (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m ctl_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class CtlcuError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+def check(status: int, ctx=None) -> None:
+    if status != OK:
+        msg = load().ctlcu_last_error(ctx).decode() if ctx else ""
+        raise CtlcuError(status, msg)

@@ -1,0 +1,791 @@
+// C ABI of the B200 forward projector: contexts, resident volumes, projection.
+//
+// Replaces the host side of CTL::OCL::RayCasterProjector
+// (modules/src/projectors/raycasterprojector.cpp) and its OpenCL runtime glue
+// (modules/src/ocl/openclconfig.cpp, pinnedmem.h): one context per device with
+// a stream and a stream-ordered memory pool; volumes uploaded once and kept
+// resident; all views of a call in one kernel launch instead of one launch,
+// one upload and one read-back per view (raycasterprojector.cpp:321-357).
+#include "ctlcu.h"
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+using namespace ctlcu;
+
+namespace {
+
+struct TexEntry {
+    cudaArray_t array = nullptr;
+    cudaTextureObject_t object = 0;
+    size_t bytes = 0;
+};
+
+struct VolumeEntry {
+    ctlcu_volume_desc desc{};
+    void* data = nullptr;       // padded storage (cudaMalloc, or pool memory when `pooled`)
+    size_t bytes = 0;
+    bool pooled = false;
+    float* mean = nullptr;      // padded 1x1x1 mean volume (f = 0), float
+    std::map<int, TexEntry> tex;  // hardware-filter copies keyed by up-sampling factor
+};
+
+}  // namespace
+
+struct ctlcu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    std::unordered_map<uint64_t, VolumeEntry> vols;
+    uint64_t next_handle = 1;
+    uint64_t budget = 0;  // 0 = unlimited
+    uint64_t used = 0;
+    int* d_flags = nullptr;
+    unsigned long long* d_counter = nullptr;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+int fail(ctlcu_ctx* ctx, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx)
+        ctx->err = buf;
+    return code;
+}
+
+#define CU_TRY(ctx, call)                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? CTLCU_ERR_OUT_OF_MEMORY          \
+                                                               : CTLCU_ERR_CUDA,                  \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                         \
+    } while (0)
+
+bool is_device_ptr(const void* p)
+{
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+size_t dtype_size(int dtype) { return dtype == CTLCU_F32 ? 4 : 2; }
+
+int check_settings(ctlcu_ctx* ctx, const ctlcu_settings* s)
+{
+    if (!s)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "settings is NULL");
+    if (s->rays_per_pixel[0] < 1 || s->rays_per_pixel[0] > 64 || s->rays_per_pixel[1] < 1 ||
+        s->rays_per_pixel[1] > 64)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "raysPerPixel must be in 1..64 (got %u, %u)",
+                    s->rays_per_pixel[0], s->rays_per_pixel[1]);
+    if (!std::isfinite(s->ray_sampling) || s->ray_sampling < 1e-3f || s->ray_sampling > 1e3f)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "raySampling must be in [1e-3, 1e3] (got %g)",
+                    (double)s->ray_sampling);
+    if (s->volume_upsampling > 64)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volumeUpSampling must be <= 64 (got %u)",
+                    s->volume_upsampling);
+    if (s->interpolate != 0 && s->interpolate != 1)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "interpolate must be 0 or 1");
+    if (s->interp_mode != CTLCU_INTERP_SOFTWARE && s->interp_mode != CTLCU_INTERP_TEXTURE)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown interp_mode %d", s->interp_mode);
+    if (s->accum < CTLCU_ACCUM_FP64 || s->accum > CTLCU_ACCUM_FP32)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown accum %d", s->accum);
+    if (s->reserved != 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "reserved must be 0");
+    return CTLCU_OK;
+}
+
+int check_desc(ctlcu_ctx* ctx, const ctlcu_volume_desc* d)
+{
+    if (!d)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume desc is NULL");
+    for (int k = 0; k < 3; ++k) {
+        if (d->n[k] == 0)
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume has no voxels (%u x %u x %u)", d->n[0],
+                        d->n[1], d->n[2]);
+        if (!(d->voxel_mm[k] > 0.0f) || !std::isfinite(d->voxel_mm[k]))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "voxel size must be positive (axis %d: %g)", k,
+                        (double)d->voxel_mm[k]);
+        if (!std::isfinite(d->offset_mm[k]))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume offset is not finite");
+    }
+    if (d->dtype < CTLCU_F32 || d->dtype > CTLCU_F16)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown dtype %d", d->dtype);
+    const uint64_t padded = (uint64_t)(d->n[0] + 2 * kPad) * (d->n[1] + 2 * kPad) * (d->n[2] + 2 * kPad);
+    if (padded >= (1ull << 31))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume too large (%llu padded voxels, limit 2^31)",
+                    (unsigned long long)padded);
+    return CTLCU_OK;
+}
+
+int check_job(ctlcu_ctx* ctx, uint32_t V, uint32_t M, uint32_t C, uint32_t R)
+{
+    if (V == 0 || M == 0 || C == 0 || R == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "empty projection job (%u views, %u modules, %ux%u)",
+                    V, M, C, R);
+    if ((uint64_t)V * M > 0x7fffffffull / 1024)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many view-modules");
+    return CTLCU_OK;
+}
+
+// Upload (or device-copy) `data` into a new zero-padded volume in the storage dtype.
+int make_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* d, const float* data, bool on_device,
+                bool pooled, VolumeEntry& v)
+{
+    const int n[3] = { (int)d->n[0], (int)d->n[1], (int)d->n[2] };
+    const size_t padded = (size_t)(n[0] + 2 * kPad) * (n[1] + 2 * kPad) * (n[2] + 2 * kPad);
+    const size_t bytes = padded * dtype_size(d->dtype);
+    if (ctx->budget && ctx->used + bytes > ctx->budget)
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY,
+                    "volume of %zu bytes exceeds the memory budget (%llu of %llu bytes used)", bytes,
+                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    v.desc = *d;
+    v.bytes = bytes;
+    v.pooled = pooled;
+    if (pooled)
+        CU_TRY(ctx, cudaMallocAsync(&v.data, bytes, ctx->stream));
+    else
+        CU_TRY(ctx, cudaMalloc(&v.data, bytes));
+    CU_TRY(ctx, cudaMemsetAsync(v.data, 0, bytes, ctx->stream));
+    const size_t nbytes = (size_t)n[0] * n[1] * n[2] * sizeof(float);
+    const float* src = data;
+    float* staging = nullptr;
+    if (!on_device) {
+        CU_TRY(ctx, cudaMallocAsync((void**)&staging, nbytes, ctx->stream));
+        CU_TRY(ctx, cudaMemcpyAsync(staging, data, nbytes, cudaMemcpyHostToDevice, ctx->stream));
+        src = staging;
+    }
+    CU_TRY(ctx, launch_pad_convert(src, v.data, n, d->dtype, ctx->stream));
+    ++ctx->launches;
+    if (staging)
+        CU_TRY(ctx, cudaFreeAsync(staging, ctx->stream));
+    ctx->used += bytes;
+    return CTLCU_OK;
+}
+
+void free_volume(ctlcu_ctx* ctx, VolumeEntry& v)
+{
+    for (auto& t : v.tex) {
+        if (t.second.object)
+            cudaDestroyTextureObject(t.second.object);
+        if (t.second.array)
+            cudaFreeArray(t.second.array);
+        ctx->used -= std::min<uint64_t>(ctx->used, t.second.bytes);
+    }
+    v.tex.clear();
+    if (v.mean)
+        cudaFreeAsync(v.mean, ctx->stream);
+    v.mean = nullptr;
+    if (v.data) {
+        if (v.pooled)
+            cudaFreeAsync(v.data, ctx->stream);
+        else
+            cudaFree(v.data);
+        ctx->used -= std::min<uint64_t>(ctx->used, v.bytes);
+    }
+    v.data = nullptr;
+}
+
+// Mean-voxel volume for volumeUpSampling = 0, computed once per volume.
+int ensure_mean(ctlcu_ctx* ctx, VolumeEntry& v)
+{
+    if (v.mean)
+        return CTLCU_OK;
+    const int n[3] = { (int)v.desc.n[0], (int)v.desc.n[1], (int)v.desc.n[2] };
+    const size_t e = 1 + 2 * kPad;
+    double* sum = nullptr;
+    CU_TRY(ctx, cudaMallocAsync((void**)&sum, sizeof(double), ctx->stream));
+    CU_TRY(ctx, cudaMemsetAsync(sum, 0, sizeof(double), ctx->stream));
+    CU_TRY(ctx, cudaMallocAsync((void**)&v.mean, e * e * e * sizeof(float), ctx->stream));
+    CU_TRY(ctx, cudaMemsetAsync(v.mean, 0, e * e * e * sizeof(float), ctx->stream));
+    CU_TRY(ctx, launch_mean(v.data, n, v.desc.dtype, sum, ctx->stream));
+    CU_TRY(ctx, launch_mean_volume(sum, (double)n[0] * n[1] * n[2], v.mean, ctx->stream));
+    ctx->launches += 2;
+    CU_TRY(ctx, cudaFreeAsync(sum, ctx->stream));
+    return CTLCU_OK;
+}
+
+// Hardware-filter texture of the volume as the rays see it (f >= 1: replicated
+// f^3; f = 0: the mean voxel).  Border colour 0, unnormalised coordinates.
+int ensure_texture(ctlcu_ctx* ctx, VolumeEntry& v, int f, cudaTextureObject_t* out)
+{
+    auto it = v.tex.find(f);
+    if (it != v.tex.end()) {
+        *out = it->second.object;
+        return CTLCU_OK;
+    }
+    if (v.desc.dtype == CTLCU_BF16)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "hardware texture interpolation supports F32 and F16 storage, not BF16");
+    int n[3] = { (int)v.desc.n[0], (int)v.desc.n[1], (int)v.desc.n[2] };
+    const void* src = v.data;
+    int dtype = v.desc.dtype;
+    int g[3];
+    if (f == 0) {
+        int r = ensure_mean(ctx, v);
+        if (r)
+            return r;
+        n[0] = n[1] = n[2] = 1;
+        src = v.mean;
+        dtype = CTLCU_F32;
+        g[0] = g[1] = g[2] = 1;
+    } else {
+        for (int k = 0; k < 3; ++k)
+            g[k] = n[k] * f;
+    }
+    const size_t esz = dtype_size(dtype);
+    const size_t bytes = (size_t)g[0] * g[1] * g[2] * esz;
+    if (ctx->budget && ctx->used + bytes > ctx->budget)
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY, "texture copy of %zu bytes exceeds the memory budget",
+                    bytes);
+    void* dense = nullptr;
+    CU_TRY(ctx, cudaMallocAsync(&dense, bytes, ctx->stream));
+    CU_TRY(ctx, launch_unpad_upsample(src, n, dtype, f == 0 ? 1 : f, dense, ctx->stream));
+    ++ctx->launches;
+    TexEntry t;
+    const cudaChannelFormatDesc ch = dtype == CTLCU_F32 ? cudaCreateChannelDesc<float>()
+                                                        : cudaCreateChannelDescHalf();
+    CU_TRY(ctx, cudaMalloc3DArray(&t.array, &ch, make_cudaExtent(g[0], g[1], g[2])));
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr(dense, g[0] * esz, g[0], g[1]);
+    p.dstArray = t.array;
+    p.extent = make_cudaExtent(g[0], g[1], g[2]);
+    p.kind = cudaMemcpyDeviceToDevice;
+    CU_TRY(ctx, cudaMemcpy3DAsync(&p, ctx->stream));
+    CU_TRY(ctx, cudaFreeAsync(dense, ctx->stream));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = t.array;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.borderColor[0] = td.borderColor[1] = td.borderColor[2] = td.borderColor[3] = 0.0f;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    CU_TRY(ctx, cudaCreateTextureObject(&t.object, &rd, &td, nullptr));
+    t.bytes = bytes;
+    ctx->used += bytes;
+    v.tex[f] = t;
+    *out = t.object;
+    return CTLCU_OK;
+}
+
+// Fill the volume-dependent part of ProjectArgs (up-sampling, step, corner).
+// Mirrors raycasterprojector.cpp:145-179 and :552-558.
+int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, ProjectArgs& a, Mode& mode,
+                int& dtype)
+{
+    const bool interp = s->interpolate != 0;
+    const int f = interp ? (int)s->volume_upsampling : 1;  // no interpolation forces f = 1
+    mode = !interp ? Mode::Nearest : (s->interp_mode == CTLCU_INTERP_TEXTURE ? Mode::Texture : Mode::Trilinear);
+    const ctlcu_volume_desc& d = v.desc;
+    float voxel[3];
+    a.tex = 0;
+    if (f == 0) {
+        int r = ensure_mean(ctx, v);
+        if (r)
+            return r;
+        for (int k = 0; k < 3; ++k) {
+            voxel[k] = d.voxel_mm[k] * (float)d.n[k];
+            a.grid[k] = 1;
+            a.ext[k] = 1 + 2 * kPad;
+        }
+        a.vol = v.mean;
+        a.up = 1;
+        dtype = CTLCU_F32;
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            voxel[k] = f == 1 ? d.voxel_mm[k] : d.voxel_mm[k] / (float)f;
+            a.grid[k] = (int)d.n[k] * f;
+            a.ext[k] = (int)d.n[k] + 2 * kPad;
+        }
+        a.vol = v.data;
+        a.up = f;
+        dtype = d.dtype;
+    }
+    if (mode == Mode::Texture) {
+        int r = ensure_texture(ctx, v, f, &a.tex);
+        if (r)
+            return r;
+    }
+    a.sy = a.ext[0];
+    a.sz = a.ext[0] * a.ext[1];
+    const float smallest = std::min(std::min(voxel[0], voxel[1]), voxel[2]);
+    a.increment = (double)smallest * (double)s->ray_sampling;
+    for (int k = 0; k < 3; ++k) {
+        a.voxel[k] = (double)voxel[k];
+        a.corner[k] = (double)d.offset_mm[k] - 0.5 * (double)a.grid[k] * a.voxel[k];
+    }
+    return CTLCU_OK;
+}
+
+void job_args(ProjectArgs& a, const ctlcu_settings* s, uint32_t V, uint32_t M, uint32_t C, uint32_t R)
+{
+    a.channels = C;
+    a.rows = R;
+    a.n_vm = V * M;
+    a.n_modules = M;
+    a.tiles_x = (C + kTileX - 1) / kTileX;
+    a.tiles_per_vm = a.tiles_x * ((R + kTileY - 1) / kTileY);
+    a.rays_x = s->rays_per_pixel[0];
+    a.rays_y = s->rays_per_pixel[1];
+}
+
+VolumeEntry* find_volume(ctlcu_ctx* ctx, uint64_t h)
+{
+    auto it = ctx->vols.find(h);
+    return it == ctx->vols.end() ? nullptr : &it->second;
+}
+
+// Setup + projection on `s` with device pmats/out.  Scratch comes from the
+// stream-ordered pool, so concurrent calls on different streams do not share it.
+int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const double* d_pm,
+                   uint32_t V, uint32_t M, uint32_t C, uint32_t R, float* d_out, cudaStream_t st)
+{
+    ProjectArgs a = {};
+    Mode mode;
+    int dtype;
+    int r = volume_args(ctx, v, s, a, mode, dtype);
+    if (r)
+        return r;
+    job_args(a, s, V, M, C, R);
+    ViewGeom* geom = nullptr;
+    CU_TRY(ctx, cudaMallocAsync((void**)&geom, sizeof(ViewGeom) * (size_t)V * M, st));
+    CU_TRY(ctx, launch_setup(d_pm, V, M, geom, nullptr, nullptr, ctx->d_flags, st));
+    a.geom = geom;
+    a.out = d_out;
+    a.flags = ctx->d_flags;
+    a.counter = nullptr;
+    CU_TRY(ctx, launch_project(a, mode, (Accum)s->accum, dtype, st));
+    ctx->launches += 2;
+    CU_TRY(ctx, cudaFreeAsync(geom, st));
+    return CTLCU_OK;
+}
+
+int read_flags(ctlcu_ctx* ctx)
+{
+    int flags = 0;
+    CU_TRY(ctx, cudaMemcpy(&flags, ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags) {
+        CU_TRY(ctx, cudaMemset(ctx->d_flags, 0, sizeof(int)));
+        if (flags & kFlagSingular)
+            return fail(ctx, CTLCU_ERR_SINGULAR_GEOMETRY,
+                        "a projection matrix has a singular or non-finite M; its pixels were set to 0");
+        return fail(ctx, CTLCU_ERR_SINGULAR_GEOMETRY, "a ray had non-finite entry/exit parameters");
+    }
+    return CTLCU_OK;
+}
+
+// Host/device dispatch shared by ctlcu_project and ctlcu_project_volume.
+int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const double* pmats,
+                uint32_t V, uint32_t M, uint32_t C, uint32_t R, float* out, cudaStream_t st,
+                bool force_sync)
+{
+    const bool pm_dev = is_device_ptr(pmats), out_dev = is_device_ptr(out);
+    const size_t pm_bytes = sizeof(double) * 12 * (size_t)V * M;
+    const size_t out_bytes = sizeof(float) * (size_t)V * M * R * C;
+    const double* d_pm = pmats;
+    double* pm_tmp = nullptr;
+    float* d_out = out;
+    if (!pm_dev || !out_dev)
+        st = ctx->stream;
+    if (!pm_dev) {
+        CU_TRY(ctx, cudaMallocAsync((void**)&pm_tmp, pm_bytes, st));
+        CU_TRY(ctx, cudaMemcpyAsync(pm_tmp, pmats, pm_bytes, cudaMemcpyHostToDevice, st));
+        d_pm = pm_tmp;
+    }
+    if (!out_dev)
+        CU_TRY(ctx, cudaMallocAsync((void**)&d_out, out_bytes, st));
+    int r = project_device(ctx, v, s, d_pm, V, M, C, R, d_out, st);
+    if (r == CTLCU_OK && !out_dev) {
+        cudaError_t e = cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess)
+            r = fail(ctx, CTLCU_ERR_CUDA, "copy of projections to the host failed: %s", cudaGetErrorString(e));
+    }
+    if (pm_tmp)
+        cudaFreeAsync(pm_tmp, st);
+    if (!out_dev)
+        cudaFreeAsync(d_out, st);
+    if (r)
+        return r;
+    if (!pm_dev || !out_dev || force_sync) {
+        CU_TRY(ctx, cudaStreamSynchronize(st));
+        return read_flags(ctx);
+    }
+    return CTLCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ctlcu_abi_version(void) { return CTLCU_ABI_VERSION; }
+
+ctlcu_settings ctlcu_settings_default(void)
+{
+    ctlcu_settings s;
+    s.rays_per_pixel[0] = s.rays_per_pixel[1] = 1;
+    s.ray_sampling = 0.3f;
+    s.volume_upsampling = 1;
+    s.interpolate = 1;
+    s.interp_mode = CTLCU_INTERP_SOFTWARE;
+    s.accum = CTLCU_ACCUM_FP64;
+    s.reserved = 0;
+    return s;
+}
+
+int ctlcu_create(int device, ctlcu_ctx** out)
+{
+    if (!out)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return CTLCU_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count)
+        return CTLCU_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess)
+        return CTLCU_ERR_CUDA;
+    ctlcu_ctx* ctx = new (std::nothrow) ctlcu_ctx;
+    if (!ctx)
+        return CTLCU_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;  // keep freed scratch in the pool between calls
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_flags, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(ctx->d_flags, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->stream)
+            cudaStreamDestroy(ctx->stream);
+        cudaFree(ctx->d_flags);
+        cudaFree(ctx->d_counter);
+        delete ctx;
+        return CTLCU_ERR_CUDA;
+    }
+    *out = ctx;
+    return CTLCU_OK;
+}
+
+int ctlcu_destroy(ctlcu_ctx* ctx)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& kv : ctx->vols)
+            free_volume(ctx, kv.second);
+        ctx->vols.clear();
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_flags);
+        cudaFree(ctx->d_counter);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return CTLCU_OK;
+}
+
+const char* ctlcu_last_error(const ctlcu_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int ctlcu_set_memory_budget(ctlcu_ctx* ctx, uint64_t bytes)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->budget = bytes;
+    return CTLCU_OK;
+}
+
+int ctlcu_memory_used(ctlcu_ctx* ctx, uint64_t* bytes)
+{
+    if (!ctx || !bytes)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *bytes = ctx->used;
+    return CTLCU_OK;
+}
+
+int ctlcu_stream(ctlcu_ctx* ctx, void** stream)
+{
+    if (!ctx || !stream)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    *stream = ctx->stream;
+    return CTLCU_OK;
+}
+
+int ctlcu_volume_create(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const float* data,
+                        int data_on_device, uint64_t* handle)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!data || !handle)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume data or handle pointer is NULL");
+    int r = check_desc(ctx, desc);
+    if (r)
+        return r;
+    cudaSetDevice(ctx->device);
+    VolumeEntry v;
+    r = make_volume(ctx, desc, data, data_on_device != 0, false, v);
+    if (r) {
+        free_volume(ctx, v);
+        return r;
+    }
+    // the caller may free or reuse `data` once this returns
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        free_volume(ctx, v);
+        return fail(ctx, CTLCU_ERR_CUDA, "volume upload failed: %s", cudaGetErrorString(e));
+    }
+    const uint64_t h = ctx->next_handle++;
+    ctx->vols.emplace(h, v);
+    *handle = h;
+    return CTLCU_OK;
+}
+
+int ctlcu_volume_release(ctlcu_ctx* ctx, uint64_t handle)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    VolumeEntry* v = find_volume(ctx, handle);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)handle);
+    cudaSetDevice(ctx->device);
+    // work already queued on other streams may still read it
+    cudaDeviceSynchronize();
+    free_volume(ctx, *v);
+    ctx->vols.erase(handle);
+    return CTLCU_OK;
+}
+
+int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes)
+{
+    if (!ctx || !bytes)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    VolumeEntry* v = find_volume(ctx, handle);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)handle);
+    uint64_t b = v->bytes;
+    for (auto& t : v->tex)
+        b += t.second.bytes;
+    *bytes = b;
+    return CTLCU_OK;
+}
+
+int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings, const double* pmats,
+                  uint32_t n_views, uint32_t n_modules, uint32_t channels, uint32_t rows, float* out,
+                  void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!pmats || !out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "pmats or out is NULL");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, n_views, n_modules, channels, rows);
+    if (r)
+        return r;
+    VolumeEntry* v = find_volume(ctx, volume);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    return project_any(ctx, *v, settings, pmats, n_views, n_modules, channels, rows, out, st, false);
+}
+
+int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const float* volume,
+                         const ctlcu_settings* settings, const double* pmats, uint32_t n_views,
+                         uint32_t n_modules, uint32_t channels, uint32_t rows, float* out)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!volume || !pmats || !out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "volume, pmats or out is NULL");
+    int r = check_desc(ctx, desc);
+    if (r)
+        return r;
+    r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, n_views, n_modules, channels, rows);
+    if (r)
+        return r;
+    cudaSetDevice(ctx->device);
+    VolumeEntry v;
+    r = make_volume(ctx, desc, volume, is_device_ptr(volume), true, v);
+    if (r == CTLCU_OK)
+        r = project_any(ctx, v, settings, pmats, n_views, n_modules, channels, rows, out, ctx->stream, true);
+    free_volume(ctx, v);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (r == CTLCU_OK && e != cudaSuccess)
+        r = fail(ctx, CTLCU_ERR_CUDA, "projection failed: %s", cudaGetErrorString(e));
+    return r;
+}
+
+int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                        const ctlcu_settings* settings, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!requests || n_requests == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "empty batch");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    for (uint32_t i = 0; i < n_requests; ++i) {
+        const ctlcu_request& q = requests[i];
+        r = check_job(ctx, q.n_views, q.n_modules, q.channels, q.rows);
+        if (r)
+            return r;
+        VolumeEntry* v = find_volume(ctx, q.volume);
+        if (!v)
+            return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "request %u: unknown volume handle %llu", i,
+                        (unsigned long long)q.volume);
+        if (!q.pmats || !q.out || !is_device_ptr(q.pmats) || !is_device_ptr(q.out))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u: pmats/out must be device memory", i);
+        r = project_device(ctx, *v, settings, q.pmats, q.n_views, q.n_modules, q.channels, q.rows, q.out, st);
+        if (r)
+            return r;
+    }
+    return CTLCU_OK;
+}
+
+int ctlcu_sync(ctlcu_ctx* ctx)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    CU_TRY(ctx, cudaDeviceSynchronize());
+    return read_flags(ctx);
+}
+
+int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                        const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,
+                        uint32_t rows, uint64_t* samples)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!pmats || !samples)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "pmats or samples is NULL");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, n_views, n_modules, channels, rows);
+    if (r)
+        return r;
+    VolumeEntry* v = find_volume(ctx, volume);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    ProjectArgs a = {};
+    Mode mode;
+    int dtype;
+    r = volume_args(ctx, *v, settings, a, mode, dtype);
+    if (r)
+        return r;
+    job_args(a, settings, n_views, n_modules, channels, rows);
+    const size_t pm_bytes = sizeof(double) * 12 * (size_t)n_views * n_modules;
+    double* d_pm = nullptr;
+    ViewGeom* geom = nullptr;
+    const bool pm_dev = is_device_ptr(pmats);
+    if (!pm_dev) {
+        CU_TRY(ctx, cudaMallocAsync((void**)&d_pm, pm_bytes, st));
+        CU_TRY(ctx, cudaMemcpyAsync(d_pm, pmats, pm_bytes, cudaMemcpyHostToDevice, st));
+    }
+    CU_TRY(ctx, cudaMallocAsync((void**)&geom, sizeof(ViewGeom) * (size_t)n_views * n_modules, st));
+    CU_TRY(ctx, launch_setup(pm_dev ? pmats : d_pm, n_views, n_modules, geom, nullptr, nullptr, ctx->d_flags, st));
+    CU_TRY(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), st));
+    a.geom = geom;
+    a.counter = ctx->d_counter;
+    a.flags = ctx->d_flags;
+    CU_TRY(ctx, launch_count(a, mode, st));
+    ctx->launches += 2;
+    unsigned long long n = 0;
+    CU_TRY(ctx, cudaMemcpyAsync(&n, ctx->d_counter, sizeof n, cudaMemcpyDeviceToHost, st));
+    CU_TRY(ctx, cudaFreeAsync(geom, st));
+    if (d_pm)
+        CU_TRY(ctx, cudaFreeAsync(d_pm, st));
+    CU_TRY(ctx, cudaStreamSynchronize(st));
+    *samples = n;
+    return read_flags(ctx);
+}
+
+int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_views, uint32_t n_modules,
+                     double* qr_out, double* src_out)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!pmats || !qr_out || !src_out || n_views == 0 || n_modules == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "bad view_setup arguments");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t nvm = (size_t)n_views * n_modules;
+    double *d_pm = nullptr, *d_qr = nullptr, *d_src = nullptr;
+    ViewGeom* geom = nullptr;
+    CU_TRY(ctx, cudaMallocAsync((void**)&d_pm, nvm * 12 * sizeof(double), st));
+    CU_TRY(ctx, cudaMallocAsync((void**)&d_qr, nvm * 15 * sizeof(double), st));
+    CU_TRY(ctx, cudaMallocAsync((void**)&d_src, (size_t)n_views * 3 * sizeof(double), st));
+    CU_TRY(ctx, cudaMallocAsync((void**)&geom, nvm * sizeof(ViewGeom), st));
+    CU_TRY(ctx, cudaMemcpyAsync(d_pm, pmats, nvm * 12 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU_TRY(ctx, launch_setup(d_pm, n_views, n_modules, geom, d_qr, d_src, nullptr, st));
+    ++ctx->launches;
+    CU_TRY(ctx, cudaMemcpyAsync(qr_out, d_qr, nvm * 15 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU_TRY(ctx, cudaMemcpyAsync(src_out, d_src, (size_t)n_views * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(d_pm, st);
+    cudaFreeAsync(d_qr, st);
+    cudaFreeAsync(d_src, st);
+    cudaFreeAsync(geom, st);
+    CU_TRY(ctx, cudaStreamSynchronize(st));
+    return CTLCU_OK;
+}
+
+int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
+{
+    if (!ctx || !launches)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *launches = ctx->launches;
+    return CTLCU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,392 @@
+// Cone-beam ray casting kernels (sm_100a).
+//
+// One thread per detector pixel; a block covers a 16x16 detector tile of one
+// (view, module), each warp an 8x4 patch.  Per ray, in FP64: direction
+// A*[x,y,1] normalised and scaled to one step in voxel units, entry/exit
+// parameters against the (half-voxel padded) volume box with the 0.01-voxel
+// face tolerance, first/last sample index.  The sample loop then runs in FP32
+// on positions rebased at the first sample, so their magnitude is bounded by
+// the volume extent rather than the source distance.
+//
+// Reference: modules/src/ocl/cl_src/projectors/raycasterprojector_interp.cl:18-148
+// (trilinear, image3d_t + CLK_FILTER_LINEAR + CLK_ADDRESS_CLAMP) and
+// raycasterprojector_no_interp.cl:16-154 (nearest voxel), launched per view
+// over (channels, rows, modules) by raycasterprojector.cpp:339-343.  Here all
+// views of a call go in one launch.
+//
+// Sampling scheme (identical to the reference): sample i sits at
+// source + i*step for i = floor(tmin) .. floor(tmax)+1, tmin/tmax clamped at
+// 0; a ray that hits no face takes no samples; the result is
+// increment * sum / raysPerPixel.  Samples outside the padded box read zeros.
+#include "internal.cuh"
+
+#include <cfloat>
+
+namespace ctlcu {
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ float load_voxel(const T* p);
+
+template <>
+__device__ __forceinline__ float load_voxel<float>(const float* p)
+{
+    return __ldg(p);
+}
+template <>
+__device__ __forceinline__ float load_voxel<__nv_bfloat16>(const __nv_bfloat16* p)
+{
+    const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));
+    return __uint_as_float(static_cast<unsigned int>(u) << 16);
+}
+template <>
+__device__ __forceinline__ float load_voxel<__half>(const __half* p)
+{
+    const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));
+    return __half2float(__ushort_as_half(u));
+}
+
+template <Accum A>
+struct Accumulator;
+
+template <>
+struct Accumulator<Accum::F64> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(float v) { s += static_cast<double>(v); }
+    __device__ __forceinline__ double value() const { return s; }
+};
+
+template <>
+struct Accumulator<Accum::Kahan> {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float v)
+    {
+        const float y = v - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return static_cast<double>(s); }
+};
+
+template <>
+struct Accumulator<Accum::F32> {
+    float s = 0.0f;
+    __device__ __forceinline__ void add(float v) { s += v; }
+    __device__ __forceinline__ double value() const { return static_cast<double>(s); }
+};
+
+// One ray ready for the sample loop.  The trilinear and texture loops run in
+// FP32 from the rounded base/step; the nearest-voxel loop keeps FP64, because a
+// position error there moves a sample into the neighbouring voxel.
+struct Ray {
+    double base[3];  // coordinate of the first sample in the loop's index space
+    double step[3];  // one step in voxel units
+    int n;           // number of samples (0: the ray misses)
+};
+
+// Face test of raycasterprojector_interp.cl:136-148.
+__device__ __forceinline__ void check_face(double h0, double h1, double lo0, double lo1, double hi0,
+                                           double hi1, double lambda, double& tmin, double& tmax)
+{
+    const bool inside = (h0 >= lo0) && (h1 >= lo1) && (h0 <= hi0) && (h1 <= hi1);
+    if (inside && lambda < tmin)
+        tmin = lambda;
+    if (inside && lambda > tmax)
+        tmax = lambda;
+}
+
+// FP64 ray setup for detector coordinate (px, py).  `shift` is added to the
+// rebased first-sample position to map it into the loop's index space.
+template <Mode M>
+__device__ __forceinline__ Ray setup_ray(const ProjectArgs& a, const ViewGeom& g, double px, double py,
+                                         int* flags)
+{
+    Ray r;
+    double d0 = g.A[0] * px + g.A[1] * py + g.A[2];
+    double d1 = g.A[3] * px + g.A[4] * py + g.A[5];
+    double d2 = g.A[6] * px + g.A[7] * py + g.A[8];
+    const double nrm = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    d0 = d0 / nrm * (a.increment / a.voxel[0]);
+    d1 = d1 / nrm * (a.increment / a.voxel[1]);
+    d2 = d2 / nrm * (a.increment / a.voxel[2]);
+    const double s0 = g.src[0] / a.voxel[0], s1 = g.src[1] / a.voxel[1], s2 = g.src[2] / a.voxel[2];
+    const double k0 = a.corner[0] / a.voxel[0], k1 = a.corner[1] / a.voxel[1],
+                 k2 = a.corner[2] / a.voxel[2];
+    const double pad = (M == Mode::Nearest) ? 0.0 : 0.5;
+    const double c10 = k0 - pad, c11 = k1 - pad, c12 = k2 - pad;
+    const double c20 = k0 + a.grid[0] + pad, c21 = k1 + a.grid[1] + pad, c22 = k2 + a.grid[2] + pad;
+    const double l10 = (c10 - s0) / d0, l11 = (c11 - s1) / d1, l12 = (c12 - s2) / d2;
+    const double l20 = (c20 - s0) / d0, l21 = (c21 - s1) / d1, l22 = (c22 - s2) / d2;
+    const double e = 0.01;
+    double tmin = DBL_MAX, tmax = 0.0;
+    check_face(s1 + l10 * d1, s2 + l10 * d2, c11 - e, c12 - e, c21 + e, c22 + e, l10, tmin, tmax);
+    check_face(s0 + l11 * d0, s2 + l11 * d2, c10 - e, c12 - e, c20 + e, c22 + e, l11, tmin, tmax);
+    check_face(s0 + l12 * d0, s1 + l12 * d1, c10 - e, c11 - e, c20 + e, c21 + e, l12, tmin, tmax);
+    check_face(s1 + l20 * d1, s2 + l20 * d2, c11 - e, c12 - e, c21 + e, c22 + e, l20, tmin, tmax);
+    check_face(s0 + l21 * d0, s2 + l21 * d2, c10 - e, c12 - e, c20 + e, c22 + e, l21, tmin, tmax);
+    check_face(s0 + l22 * d0, s1 + l22 * d1, c10 - e, c11 - e, c20 + e, c21 + e, l22, tmin, tmax);
+    r.n = 0;
+    if (tmin == DBL_MAX) {
+        r.base[0] = r.base[1] = r.base[2] = 0.0;
+        r.step[0] = r.step[1] = r.step[2] = 0.0;
+        return r;
+    }
+    const double t0 = fmax(tmin, 0.0), t1 = fmax(tmax, 0.0);
+    // the box diagonal bounds any honest ray; beyond it the inputs are broken
+    if (!(t1 - t0 < 1.0e7) || !isfinite(t0)) {
+        if (flags)
+            atomicOr(flags, kFlagNonFinite);
+        r.n = 0;
+        r.base[0] = r.base[1] = r.base[2] = 0.0;
+        r.step[0] = r.step[1] = r.step[2] = 0.0;
+        return r;
+    }
+    const double i0 = floor(t0), i1 = floor(t1) + 1.0;
+    r.n = static_cast<int>(i1 - i0) + 1;
+    // position relative to the corner: (source - corner) + i * step
+    double shift;
+    if (M == Mode::Trilinear)
+        shift = (a.up == 1) ? (kPad - 0.5) : -0.5;  // taps at floor(p - 0.5) (+ pad)
+    else if (M == Mode::Nearest)
+        shift = kPad;                                // voxel floor(p) (+ pad)
+    else
+        shift = 0.0;                                 // texture: hardware subtracts 0.5
+    r.base[0] = (s0 - k0) + i0 * d0 + shift;
+    r.base[1] = (s1 - k1) + i0 * d1 + shift;
+    r.base[2] = (s2 - k2) + i0 * d2 + shift;
+    r.step[0] = d0;
+    r.step[1] = d1;
+    r.step[2] = d2;
+    return r;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+__device__ __forceinline__ int floor_div(int i, int f) { return i >= 0 ? i / f : -((f - 1 - i) / f); }
+
+// Sample loop, trilinear with zero border, volume stored as T (padded).
+template <typename T, Accum ACC, bool UP>
+__device__ __forceinline__ void march_trilinear(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
+{
+    const T* __restrict__ vol = static_cast<const T*>(a.vol);
+    const int sy = a.sy, sz = a.sz;
+    const int mx = a.ext[0] - 2, my = a.ext[1] - 2, mz = a.ext[2] - 2;
+    const float bx = (float)r.base[0], by = (float)r.base[1], bz = (float)r.base[2];
+    const float dx = (float)r.step[0], dy = (float)r.step[1], dz = (float)r.step[2];
+    for (int k = 0; k < r.n; ++k) {
+        const float kf = static_cast<float>(k);
+        const float ux = fmaf(kf, dx, bx);
+        const float uy = fmaf(kf, dy, by);
+        const float uz = fmaf(kf, dz, bz);
+        const float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+        const float wx = ux - fx, wy = uy - fy, wz = uz - fz;
+        float v000, v100, v010, v110, v001, v101, v011, v111;
+        if (!UP) {
+            const int ix = clampi(__float2int_rz(fx), 0, mx);
+            const int iy = clampi(__float2int_rz(fy), 0, my);
+            const int iz = clampi(__float2int_rz(fz), 0, mz);
+            const T* p = vol + (ix + iy * sy + iz * sz);
+            v000 = load_voxel(p);
+            v100 = load_voxel(p + 1);
+            v010 = load_voxel(p + sy);
+            v110 = load_voxel(p + sy + 1);
+            v001 = load_voxel(p + sz);
+            v101 = load_voxel(p + sz + 1);
+            v011 = load_voxel(p + sz + sy);
+            v111 = load_voxel(p + sz + sy + 1);
+        } else {
+            // virtual replication: grid index g maps to stored voxel floor(g / f)
+            const int f = a.up;
+            const int gx = __float2int_rz(fmaxf(fminf(fx, 1.0e8f), -1.0e8f));
+            const int gy = __float2int_rz(fmaxf(fminf(fy, 1.0e8f), -1.0e8f));
+            const int gz = __float2int_rz(fmaxf(fminf(fz, 1.0e8f), -1.0e8f));
+            const int x0 = clampi(floor_div(gx, f) + kPad, 0, mx + 1);
+            const int x1 = clampi(floor_div(gx + 1, f) + kPad, 0, mx + 1);
+            const int y0 = clampi(floor_div(gy, f) + kPad, 0, my + 1) * sy;
+            const int y1 = clampi(floor_div(gy + 1, f) + kPad, 0, my + 1) * sy;
+            const int z0 = clampi(floor_div(gz, f) + kPad, 0, mz + 1) * sz;
+            const int z1 = clampi(floor_div(gz + 1, f) + kPad, 0, mz + 1) * sz;
+            v000 = load_voxel(vol + (x0 + y0 + z0));
+            v100 = load_voxel(vol + (x1 + y0 + z0));
+            v010 = load_voxel(vol + (x0 + y1 + z0));
+            v110 = load_voxel(vol + (x1 + y1 + z0));
+            v001 = load_voxel(vol + (x0 + y0 + z1));
+            v101 = load_voxel(vol + (x1 + y0 + z1));
+            v011 = load_voxel(vol + (x0 + y1 + z1));
+            v111 = load_voxel(vol + (x1 + y1 + z1));
+        }
+        const float c00 = fmaf(wx, v100 - v000, v000);
+        const float c10 = fmaf(wx, v110 - v010, v010);
+        const float c01 = fmaf(wx, v101 - v001, v001);
+        const float c11 = fmaf(wx, v111 - v011, v011);
+        const float c0 = fmaf(wy, c10 - c00, c00);
+        const float c1 = fmaf(wy, c11 - c01, c01);
+        acc.add(fmaf(wz, c1 - c0, c0));
+    }
+}
+
+// Sample loop, nearest voxel floor(p) with bounds test (zeros outside).
+template <typename T, Accum ACC>
+__device__ __forceinline__ void march_nearest(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
+{
+    const T* __restrict__ vol = static_cast<const T*>(a.vol);
+    const int mx = a.ext[0] - 1, my = a.ext[1] - 1, mz = a.ext[2] - 1;
+    for (int k = 0; k < r.n; ++k) {
+        const double kd = static_cast<double>(k);
+        const double px = fmin(fmax(fma(kd, r.step[0], r.base[0]), -1.0), 1.0e9);
+        const double py = fmin(fmax(fma(kd, r.step[1], r.base[1]), -1.0), 1.0e9);
+        const double pz = fmin(fmax(fma(kd, r.step[2], r.base[2]), -1.0), 1.0e9);
+        const int ix = clampi(__double2int_rd(px), 0, mx);
+        const int iy = clampi(__double2int_rd(py), 0, my);
+        const int iz = clampi(__double2int_rd(pz), 0, mz);
+        acc.add(load_voxel(vol + (ix + iy * a.sy + iz * a.sz)));
+    }
+}
+
+// Sample loop, hardware texture filter (border colour 0, unnormalised coords).
+template <Accum ACC>
+__device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
+{
+    const float bx = (float)r.base[0], by = (float)r.base[1], bz = (float)r.base[2];
+    const float dx = (float)r.step[0], dy = (float)r.step[1], dz = (float)r.step[2];
+    for (int k = 0; k < r.n; ++k) {
+        const float kf = static_cast<float>(k);
+        acc.add(tex3D<float>(a.tex, fmaf(kf, dx, bx), fmaf(kf, dy, by), fmaf(kf, dz, bz)));
+    }
+}
+
+__device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
+{
+    const uint32_t b = blockIdx.x;
+    vm = b / a.tiles_per_vm;
+    const uint32_t t = b - vm * a.tiles_per_vm;
+    const uint32_t ty = t / a.tiles_x, tx = t - ty * a.tiles_x;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    x = tx * kTileX + (warp & 1u) * 8u + (lane & 7u);
+    y = ty * kTileY + (warp >> 1) * 4u + (lane >> 3);
+    return x < a.channels && y < a.rows;
+}
+
+template <typename T, Mode M, Accum ACC, bool UP>
+__global__ void __launch_bounds__(kBlock) project_kernel(const ProjectArgs a)
+{
+    uint32_t vm, x, y;
+    if (!pixel_of(a, vm, x, y))
+        return;
+    const ViewGeom& g = a.geom[vm];
+    float* dst = a.out + ((size_t)vm * a.rows + y) * a.channels + x;
+    if (!g.valid) {
+        *dst = 0.0f;
+        return;
+    }
+    Accumulator<ACC> acc;
+    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+            const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
+            const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
+            const Ray r = setup_ray<M>(a, g, px, py, a.flags);
+            if (M == Mode::Trilinear)
+                march_trilinear<T, ACC, UP>(a, r, acc);
+            else if (M == Mode::Nearest)
+                march_nearest<T, ACC>(a, r, acc);
+            else
+                march_texture<ACC>(a, r, acc);
+        }
+    *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
+}
+
+template <Mode M>
+__global__ void __launch_bounds__(kBlock) count_kernel(const ProjectArgs a)
+{
+    uint32_t vm, x, y;
+    unsigned long long n = 0;
+    if (pixel_of(a, vm, x, y)) {
+        const ViewGeom& g = a.geom[vm];
+        if (g.valid) {
+            const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+            for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+                for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+                    const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
+                    const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
+                    n += (unsigned long long)setup_ray<M>(a, g, px, py, nullptr).n;
+                }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31u) == 0 && n)
+        atomicAdd(a.counter, n);
+}
+
+template <Mode M, Accum ACC, bool UP>
+cudaError_t launch_typed(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
+{
+    switch (dtype) {
+    case 0: project_kernel<float, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
+    case 1: project_kernel<__nv_bfloat16, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
+    case 2: project_kernel<__half, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <Mode M, Accum ACC>
+cudaError_t launch_mode(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
+{
+    if (M == Mode::Texture) {
+        project_kernel<float, Mode::Texture, ACC, false><<<grid, kBlock, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+    if (M == Mode::Trilinear && a.up != 1)
+        return launch_typed<M, ACC, true>(a, dtype, grid, s);
+    return launch_typed<M, ACC, false>(a, dtype, grid, s);
+}
+
+template <Accum ACC>
+cudaError_t launch_acc(const ProjectArgs& a, Mode mode, int dtype, dim3 grid, cudaStream_t s)
+{
+    switch (mode) {
+    case Mode::Trilinear: return launch_mode<Mode::Trilinear, ACC>(a, dtype, grid, s);
+    case Mode::Nearest: return launch_mode<Mode::Nearest, ACC>(a, dtype, grid, s);
+    case Mode::Texture: return launch_mode<Mode::Texture, ACC>(a, dtype, grid, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype, cudaStream_t s)
+{
+    const uint64_t blocks = (uint64_t)a.n_vm * a.tiles_per_vm;
+    if (blocks == 0)
+        return cudaSuccess;
+    if (blocks > 0x7fffffffull)
+        return cudaErrorInvalidConfiguration;
+    const dim3 grid((unsigned)blocks);
+    switch (acc) {
+    case Accum::F64: return launch_acc<Accum::F64>(a, mode, dtype, grid, s);
+    case Accum::Kahan: return launch_acc<Accum::Kahan>(a, mode, dtype, grid, s);
+    case Accum::F32: return launch_acc<Accum::F32>(a, mode, dtype, grid, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_count(const ProjectArgs& a, Mode mode, cudaStream_t s)
+{
+    const uint64_t blocks = (uint64_t)a.n_vm * a.tiles_per_vm;
+    if (blocks == 0)
+        return cudaSuccess;
+    if (blocks > 0x7fffffffull)
+        return cudaErrorInvalidConfiguration;
+    const dim3 grid((unsigned)blocks);
+    if (mode == Mode::Nearest)
+        count_kernel<Mode::Nearest><<<grid, kBlock, 0, s>>>(a);
+    else
+        count_kernel<Mode::Trilinear><<<grid, kBlock, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace ctlcu

@@ -1,0 +1,460 @@
+"""Host-side interface of the B200 projector, mirroring CTL's projector API.
+
+``CudaRayCasterProjector`` has the method names, settings, parameter keys and
+error behaviour of ``CTL::OCL::RayCasterProjector``
+(modules/src/projectors/raycasterprojector.h:20-58, raycasterprojector.cpp)
+and of the ``AbstractProjector`` interface it implements
+(modules/src/projectors/abstractprojector.h:65-144):
+
+  configure(setup)            stores the projection matrices and view dimensions
+  project(volume)             -> ProjectionData [view][module][row][channel]
+  project_composite(volumes)  sum of the sub-volume projections
+  is_linear()                 True
+  parameter() / set_parameter(map) with the reference's keys
+  to_variant() / from_variant(map)
+  settings()                  the Settings object (raysPerPixel, raySampling, ...)
+  notifier                    callbacks receiving projectionFinished(view)
+
+``Context`` is the thin, lower-level handle on one device (resident volumes,
+device-pointer projection, batches) that the projector and the benchmark use.
+Both call the C ABI in libctlcu.so; nothing here computes projections itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import logging
+import math
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+log = logging.getLogger("ctl_b200")
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if _is_torch(x):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def _contig_f64(x):
+    if _is_torch(x):
+        import torch
+        return x.to(torch.float64).contiguous()
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _contig_f32(x):
+    if _is_torch(x):
+        import torch
+        return x.to(torch.float32).contiguous()
+    return np.ascontiguousarray(x, dtype=np.float32)
+
+
+def _is_cuda(x) -> bool:
+    return _is_torch(x) and x.is_cuda
+
+
+# ---------------------------------------------------------------------------------------------
+# settings, volumes, projection data
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class Settings:
+    """RayCasterProjector::Settings (raycasterprojector.h:27-37) plus the B200 options."""
+    device_ids: List[int] = field(default_factory=list)
+    rays_per_pixel: List[int] = field(default_factory=lambda: [1, 1])
+    ray_sampling: float = 0.3
+    volume_upsampling: int = 1
+    interpolate: bool = True
+    interp_mode: int = L.INTERP_SOFTWARE
+    accum: int = L.ACCUM_FP64
+    storage: int = L.F32
+
+    def to_c(self) -> L.Settings:
+        s = L.Settings()
+        s.rays_per_pixel[0] = int(self.rays_per_pixel[0])
+        s.rays_per_pixel[1] = int(self.rays_per_pixel[1])
+        s.ray_sampling = float(self.ray_sampling)
+        s.volume_upsampling = int(self.volume_upsampling)
+        s.interpolate = 1 if self.interpolate else 0
+        s.interp_mode = int(self.interp_mode)
+        s.accum = int(self.accum)
+        s.reserved = 0
+        return s
+
+    @staticmethod
+    def optimized_for(smallest_voxel_mm: float, pixel_dims_mm: Sequence[float]) -> "Settings":
+        """Settings::optimizedFor (raycasterprojector.cpp:482-521): rays per pixel
+        for rectangular pixels, an up-sampling factor for voxels larger than the
+        pixels, more rays for voxels smaller than the pixels."""
+        ret = Settings()
+        xmm, ymm = float(pixel_dims_mm[0]), float(pixel_dims_mm[1])
+        if xmm == 0.0 or ymm == 0.0:
+            raise RuntimeError("pixel dimensions are singular")
+        ratio = xmm / ymm
+        broad = ratio > 1.0
+        if broad:
+            ratio = 1.0 / ratio
+        deviation = abs(ratio - 1.0)
+        for r in ((1, 2), (1, 3), (1, 4), (2, 3), (3, 4)):
+            if abs(ratio - r[0] / r[1]) < deviation:
+                deviation = abs(ratio - r[0] / r[1])
+                ret.rays_per_pixel = [r[1] if broad else r[0], r[0] if broad else r[1]]
+        smallest_pixel = min(xmm / ret.rays_per_pixel[0], ymm / ret.rays_per_pixel[1])
+        ret.volume_upsampling = max(int(smallest_voxel_mm / smallest_pixel), 1)
+        inc = max(int(smallest_pixel / smallest_voxel_mm), 1)
+        ret.rays_per_pixel = [ret.rays_per_pixel[0] * inc, ret.rays_per_pixel[1] * inc]
+        return ret
+
+
+@dataclass
+class VoxelVolume:
+    """Float32 volume, numpy (Z, Y, X) or torch tensor, x fastest; sizes in mm."""
+    data: object
+    voxel_size: Sequence[float]
+    offset: Sequence[float] = (0.0, 0.0, 0.0)
+
+    def has_data(self) -> bool:
+        return self.data is not None and int(np.prod(tuple(self.data.shape))) > 0
+
+    def nb_voxels(self):
+        z, y, x = tuple(self.data.shape)
+        return int(x), int(y), int(z)
+
+    def smallest_voxel_size(self) -> float:
+        return float(min(self.voxel_size))
+
+    def desc(self, dtype: int = L.F32) -> L.VolumeDesc:
+        d = L.VolumeDesc()
+        nx, ny, nz = self.nb_voxels()
+        d.n[0], d.n[1], d.n[2] = nx, ny, nz
+        for k in range(3):
+            d.voxel_mm[k] = float(self.voxel_size[k])
+            d.offset_mm[k] = float(self.offset[k])
+        d.dtype = int(dtype)
+        return d
+
+
+@dataclass
+class ViewDimensions:
+    """SingleViewData::Dimensions: channels, rows, modules."""
+    nb_channels: int
+    nb_rows: int
+    nb_modules: int
+
+
+@dataclass
+class AcquisitionGeometry:
+    """What configure() extracts from an AcquisitionSetup: the FullGeometry
+    (views x modules projection matrices) and the view dimensions
+    (raycasterprojector.cpp:97-107)."""
+    pmats: np.ndarray           # (views, modules, 3, 4) float64
+    view_dim: ViewDimensions
+
+
+class ProjectionData:
+    """[view][module] images of rows x channels, float32 (projectiondata.h:19-95)."""
+
+    def __init__(self, view_dim: ViewDimensions, data=None):
+        self.view_dim = view_dim
+        if data is None:
+            data = np.zeros((0, view_dim.nb_modules, view_dim.nb_rows, view_dim.nb_channels), np.float32)
+        self.data = data
+
+    def nb_views(self) -> int:
+        return int(self.data.shape[0])
+
+    def view(self, v):
+        return self.data[v]
+
+    def module(self, v, m):
+        return self.data[v, m]
+
+    def numpy(self) -> np.ndarray:
+        if _is_torch(self.data):
+            return self.data.detach().cpu().numpy()
+        return np.asarray(self.data)
+
+    def __iadd__(self, other: "ProjectionData"):
+        self.data = self.data + other.data
+        return self
+
+    def __add__(self, other: "ProjectionData"):
+        return ProjectionData(self.view_dim, self.data + other.data)
+
+
+# ---------------------------------------------------------------------------------------------
+# context
+# ---------------------------------------------------------------------------------------------
+
+class Volume:
+    """A volume resident in device memory (handle on a Context)."""
+
+    def __init__(self, ctx: "Context", handle: int, desc: L.VolumeDesc):
+        self.ctx = ctx
+        self.handle = handle
+        self.desc = desc
+
+    @property
+    def nbytes(self) -> int:
+        b = C.c_uint64(0)
+        self.ctx._check(self.ctx.lib.ctlcu_volume_bytes(self.ctx.h, self.handle, C.byref(b)))
+        return int(b.value)
+
+    def release(self) -> None:
+        if self.handle:
+            self.ctx._check(self.ctx.lib.ctlcu_volume_release(self.ctx.h, self.handle))
+            self.handle = 0
+
+
+class Context:
+    """One CUDA device: stream, memory budget, resident volumes, projection calls."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        L.check(self.lib.ctlcu_create(int(device), C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.ctlcu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int) -> None:
+        L.check(status, self.h)
+
+    # ---- memory ---------------------------------------------------------------------------
+    def set_memory_budget(self, nbytes: int) -> None:
+        self._check(self.lib.ctlcu_set_memory_budget(self.h, int(nbytes)))
+
+    def memory_used(self) -> int:
+        b = C.c_uint64(0)
+        self._check(self.lib.ctlcu_memory_used(self.h, C.byref(b)))
+        return int(b.value)
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self.lib.ctlcu_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def launches(self) -> int:
+        n = C.c_uint64(0)
+        self._check(self.lib.ctlcu_launch_count(self.h, C.byref(n)))
+        return int(n.value)
+
+    # ---- volumes --------------------------------------------------------------------------
+    def volume(self, vol: VoxelVolume, dtype: int = L.F32) -> Volume:
+        data = _contig_f32(vol.data)
+        desc = vol.desc(dtype)
+        h = C.c_uint64(0)
+        self._check(self.lib.ctlcu_volume_create(self.h, C.byref(desc), C.c_void_p(_ptr(data)),
+                                                 1 if _is_cuda(data) else 0, C.byref(h)))
+        return Volume(self, int(h.value), desc)
+
+    # ---- projection -----------------------------------------------------------------------
+    @staticmethod
+    def _out_like(pmats, V, M, R, Cn):
+        if _is_cuda(pmats):
+            import torch
+            return torch.empty((V, M, R, Cn), dtype=torch.float32, device=pmats.device)
+        return np.empty((V, M, R, Cn), dtype=np.float32)
+
+    def project(self, volume: Volume, pmats, channels: int, rows: int,
+                settings: Optional[Settings] = None, out=None, stream: int = 0):
+        settings = settings or Settings()
+        P = _contig_f64(pmats)
+        V, M = int(P.shape[0]), int(P.shape[1])
+        if out is None:
+            out = self._out_like(P, V, M, rows, channels)
+        st = settings.to_c()
+        self._check(self.lib.ctlcu_project(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(P)), V, M,
+                                           int(channels), int(rows), C.c_void_p(_ptr(out)),
+                                           C.c_void_p(stream or None)))
+        return out
+
+    def project_volume(self, vol: VoxelVolume, pmats, channels: int, rows: int,
+                       settings: Optional[Settings] = None, out=None):
+        """One-shot: upload, project, release (the reference's per-call semantics)."""
+        settings = settings or Settings()
+        data = _contig_f32(vol.data)
+        P = _contig_f64(pmats)
+        V, M = int(P.shape[0]), int(P.shape[1])
+        if out is None:
+            out = self._out_like(P, V, M, rows, channels)
+        desc = vol.desc(settings.storage)
+        st = settings.to_c()
+        self._check(self.lib.ctlcu_project_volume(self.h, C.byref(desc), C.c_void_p(_ptr(data)), C.byref(st),
+                                                  C.c_void_p(_ptr(P)), V, M, int(channels), int(rows),
+                                                  C.c_void_p(_ptr(out))))
+        return out
+
+    def project_batch(self, requests: Sequence[tuple], settings: Optional[Settings] = None,
+                      stream: int = 0) -> None:
+        """requests: (Volume, device pmats tensor (V,M,3,4) f64, device out tensor (V,M,R,C) f32)."""
+        settings = settings or Settings()
+        arr = (L.Request * len(requests))()
+        for i, (vol, P, out) in enumerate(requests):
+            arr[i].volume = vol.handle
+            arr[i].pmats = _ptr(P)
+            arr[i].out = _ptr(out)
+            arr[i].n_views, arr[i].n_modules = int(P.shape[0]), int(P.shape[1])
+            arr[i].rows, arr[i].channels = int(out.shape[2]), int(out.shape[3])
+        st = settings.to_c()
+        self._check(self.lib.ctlcu_project_batch(self.h, arr, len(requests), C.byref(st),
+                                                 C.c_void_p(stream or None)))
+
+    def sync(self) -> None:
+        self._check(self.lib.ctlcu_sync(self.h))
+
+    def count_samples(self, volume: Volume, pmats, channels: int, rows: int,
+                      settings: Optional[Settings] = None) -> int:
+        settings = settings or Settings()
+        P = _contig_f64(pmats)
+        n = C.c_uint64(0)
+        st = settings.to_c()
+        self._check(self.lib.ctlcu_count_samples(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(P)),
+                                                 int(P.shape[0]), int(P.shape[1]), int(channels), int(rows),
+                                                 C.byref(n)))
+        return int(n.value)
+
+    def view_setup(self, pmats):
+        P = np.ascontiguousarray(pmats, dtype=np.float64)
+        V, M = P.shape[0], P.shape[1]
+        qr = np.zeros((V, M, 15))
+        src = np.zeros((V, 3))
+        self._check(self.lib.ctlcu_view_setup(self.h, C.c_void_p(P.ctypes.data), V, M,
+                                              C.c_void_p(qr.ctypes.data), C.c_void_p(src.ctypes.data)))
+        return qr, src
+
+
+# ---------------------------------------------------------------------------------------------
+# the AbstractProjector mirror
+# ---------------------------------------------------------------------------------------------
+
+class CudaRayCasterProjector:
+    """Drop-in for CTL::OCL::RayCasterProjector on one B200."""
+
+    TYPE_ID = 1  # CTL_TYPE_ID(1) of RayCasterProjector (raycasterprojector.h:22)
+
+    def __init__(self, device: int = 0):
+        # the reference constructor throws when OpenCL or its kernels are
+        # missing (raycasterprojector.cpp:388-422); here loading the library
+        # or binding the device raises
+        self._settings = Settings()
+        self._ctx = Context(device)
+        self._geometry: Optional[AcquisitionGeometry] = None
+        self.notifier: List[Callable[[int], None]] = []
+
+    # ---- AbstractProjector ----------------------------------------------------------------
+    def configure(self, setup: AcquisitionGeometry) -> None:
+        """raycasterprojector.cpp:97-107"""
+        P = np.ascontiguousarray(setup.pmats, dtype=np.float64)
+        if P.ndim != 4 or P.shape[2:] != (3, 4) or P.shape[1] != setup.view_dim.nb_modules:
+            raise ValueError("FullGeometry must be (views, modules, 3, 4) with modules = nbModules")
+        self._geometry = AcquisitionGeometry(P, setup.view_dim)
+
+    def project(self, volume: VoxelVolume) -> ProjectionData:
+        """raycasterprojector.cpp:139-375.  An invalid volume logs an error and
+        returns empty ProjectionData; a device error logs and returns the
+        (zero) result, as the reference does."""
+        if self._geometry is None:
+            raise RuntimeError("CudaRayCasterProjector::project: configure() has not been called")
+        vd = self._geometry.view_dim
+        ret = ProjectionData(vd)
+        if not self._settings.interpolate:
+            self._settings.volume_upsampling = 1
+        if not volume.has_data():
+            log.critical("no or contradictory data in volume object")
+            return ret
+        if volume.smallest_voxel_size() <= 0.0:
+            log.warning("voxel size is zero or negative")
+        P = self._geometry.pmats
+        try:
+            out = self._ctx.project_volume(volume, P, vd.nb_channels, vd.nb_rows, self._settings)
+            ret.data = out
+        except L.CtlcuError as e:
+            log.critical("ctlcu error: %s", e)
+            if e.status == L.ERR_SINGULAR_GEOMETRY:
+                pass
+            ret.data = np.zeros((P.shape[0], vd.nb_modules, vd.nb_rows, vd.nb_channels), np.float32)
+        for v in range(P.shape[0]):
+            for cb in self.notifier:
+                cb(v)
+        return ret
+
+    def project_composite(self, volumes: Sequence[VoxelVolume]) -> ProjectionData:
+        """AbstractProjector::projectComposite (abstractprojector.h:99-112)."""
+        if len(volumes) == 0:
+            raise RuntimeError("AbstractProjector::projectComposite: Volume is empty.")
+        ret = self.project(volumes[0])
+        for v in volumes[1:]:
+            ret += self.project(v)
+        return ret
+
+    def is_linear(self) -> bool:
+        return True
+
+    # ---- parameters / serialisation (raycasterprojector.cpp:60-91) --------------------------
+    def parameter(self) -> dict:
+        s = self._settings
+        return {
+            "Rays per pixel X": int(s.rays_per_pixel[0]),
+            "Rays per pixel Y": int(s.rays_per_pixel[1]),
+            "Ray sampling step length": float(s.ray_sampling),
+            "Volume upsampling factor": int(s.volume_upsampling),
+            "Interpolate": bool(s.interpolate),
+            "Interpolation mode": "texture" if s.interp_mode == L.INTERP_TEXTURE else "software",
+            "Accumulation": {L.ACCUM_FP64: "fp64", L.ACCUM_KAHAN: "kahan", L.ACCUM_FP32: "fp32"}[s.accum],
+            "Storage": {L.F32: "f32", L.BF16: "bf16", L.F16: "f16"}[s.storage],
+        }
+
+    def set_parameter(self, parameter: dict) -> None:
+        m = dict(parameter)
+        s = self._settings
+        s.rays_per_pixel = [int(m.get("Rays per pixel X", 1)), int(m.get("Rays per pixel Y", 1))]
+        s.ray_sampling = float(m.get("Ray sampling step length", 0.3))
+        s.volume_upsampling = int(m.get("Volume upsampling factor", 1))
+        s.interpolate = bool(m.get("Interpolate", True))
+        s.interp_mode = L.INTERP_TEXTURE if m.get("Interpolation mode", "software") == "texture" \
+            else L.INTERP_SOFTWARE
+        s.accum = {"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[
+            m.get("Accumulation", "fp64")]
+        s.storage = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[m.get("Storage", "f32")]
+
+    def to_variant(self) -> dict:
+        return {"type-id": self.TYPE_ID, "#": "CudaRayCasterProjector", "parameters": self.parameter()}
+
+    def from_variant(self, variant: dict) -> None:
+        self.set_parameter(variant.get("parameters", {}))
+
+    def settings(self) -> Settings:
+        return self._settings
+
+    @property
+    def context(self) -> Context:
+        return self._ctx

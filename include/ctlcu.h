@@ -1,0 +1,184 @@
+/*
+ * ctlcu -- C ABI of the B200 cone-beam forward projector.
+ *
+ * A drop-in for CTL's OpenCL forward projector CTL::OCL::RayCasterProjector
+ * (modules/src/projectors/raycasterprojector.h:20-58).  The C++ adapter
+ * CudaRayCasterProjector (ctl_b200/adapter/) implements CTL's AbstractProjector
+ * on top of these calls; the Python package ctl_b200 binds them with ctypes.
+ *
+ * Conventions
+ *   - every call returns a ctlcu_status (0 = OK) and never throws;
+ *     ctlcu_last_error() gives a readable message for the last failure on a
+ *     context (thread-local to the context's lock holder, valid until the next
+ *     call on that context);
+ *   - a context owns one CUDA device, a CUDA stream and the volumes created on
+ *     it; all calls on a context are serialised by an internal lock;
+ *   - projection matrices are 3x4 row-major float64, ordered
+ *     [view][module] (CTL's FullGeometry, acquisition/geometryencoder.h);
+ *   - projections are float32 [view][module][row][channel] (CTL's
+ *     ProjectionData / Chunk2D layout, img/projectiondata.h:19-95,
+ *     img/chunk2d.tpp:477-492);
+ *   - volumes are float32 on the host, x fastest, index z*X*Y + y*X + x
+ *     (img/voxelvolume.tpp:310-335), centred at offset_mm.
+ */
+#ifndef CTLCU_H
+#define CTLCU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTLCU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CTLCU_API __attribute__((visibility("default")))
+#else
+#define CTLCU_API
+#endif
+
+typedef enum {
+    CTLCU_OK = 0,
+    CTLCU_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size or setting */
+    CTLCU_ERR_INVALID_HANDLE = 2,   /* unknown or released volume handle */
+    CTLCU_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed or memory budget exceeded */
+    CTLCU_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    CTLCU_ERR_NO_DEVICE = 5,        /* device index out of range / no CUDA device */
+    CTLCU_ERR_SINGULAR_GEOMETRY = 6,/* a projection matrix had a singular M; its pixels are 0 */
+    CTLCU_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+    CTLCU_ERR_BUSY = 8              /* admission refused (queue full) */
+} ctlcu_status;
+
+typedef enum { CTLCU_F32 = 0, CTLCU_BF16 = 1, CTLCU_F16 = 2 } ctlcu_dtype;
+
+typedef enum {
+    CTLCU_INTERP_SOFTWARE = 0, /* FP32 trilinear from the stored volume (default) */
+    CTLCU_INTERP_TEXTURE = 1   /* hardware texture filter (8-bit fractional weights) */
+} ctlcu_interp_mode;
+
+typedef enum {
+    CTLCU_ACCUM_FP64 = 0,  /* double accumulator, as raycasterprojector_interp.cl:48,66 */
+    CTLCU_ACCUM_KAHAN = 1, /* float with compensated (Kahan) summation */
+    CTLCU_ACCUM_FP32 = 2   /* plain float */
+} ctlcu_accum;
+
+typedef struct ctlcu_ctx ctlcu_ctx;
+
+typedef struct {
+    uint32_t n[3];       /* voxels along x, y, z */
+    float voxel_mm[3];   /* VoxelVolume::voxelSize() */
+    float offset_mm[3];  /* VoxelVolume::offset() */
+    int32_t dtype;       /* ctlcu_dtype used for device storage (host data is float32) */
+} ctlcu_volume_desc;
+
+/*
+ * RayCasterProjector::Settings (raycasterprojector.h:27-37) plus the
+ * B200 options.  ctlcu_settings_default() gives the reference defaults:
+ * rays {1,1}, raySampling 0.3, volumeUpSampling 1, interpolate on,
+ * software interpolation, FP64 accumulation.
+ */
+typedef struct {
+    uint32_t rays_per_pixel[2]; /* sub-rays along channel (x) and row (y), 1..64 */
+    float ray_sampling;         /* step / smallest voxel size, >= 1e-3 */
+    uint32_t volume_upsampling; /* 0: one mean voxel, 1: as is, f>=2: f^3 replication (virtual) */
+    int32_t interpolate;        /* 1 trilinear, 0 nearest voxel (forces up-sampling 1) */
+    int32_t interp_mode;        /* ctlcu_interp_mode */
+    int32_t accum;              /* ctlcu_accum */
+    int32_t reserved;           /* must be 0 */
+} ctlcu_settings;
+
+/* One projection request of a batch: device pointers, see ctlcu_project_batch. */
+typedef struct {
+    uint64_t volume;       /* handle from ctlcu_volume_create */
+    const double* pmats;   /* device: n_views*n_modules*12 doubles */
+    float* out;            /* device: n_views*n_modules*rows*channels floats */
+    uint32_t n_views, n_modules, channels, rows;
+} ctlcu_request;
+
+/* ---- context ---------------------------------------------------------------------------- */
+
+/* Replaces OpenCLConfig::instance() + RayCasterProjector::initOpenCL
+ * (ocl/openclconfig.cpp:15-38, raycasterprojector.cpp:388-422): binds one CUDA
+ * device.  Fails with CTLCU_ERR_NO_DEVICE for a bad index, like
+ * prepareOpenCLDeviceList (raycasterprojector.cpp:434-461). */
+CTLCU_API int ctlcu_create(int device, ctlcu_ctx** out);
+CTLCU_API int ctlcu_destroy(ctlcu_ctx* ctx);
+CTLCU_API const char* ctlcu_last_error(const ctlcu_ctx* ctx);
+CTLCU_API int ctlcu_abi_version(void);
+CTLCU_API ctlcu_settings ctlcu_settings_default(void);
+
+/* Device-memory budget for volumes (bytes, 0 = unlimited).  Creating a volume
+ * beyond it fails with CTLCU_ERR_OUT_OF_MEMORY. */
+CTLCU_API int ctlcu_set_memory_budget(ctlcu_ctx* ctx, uint64_t bytes);
+CTLCU_API int ctlcu_memory_used(ctlcu_ctx* ctx, uint64_t* bytes);
+
+/* The context's CUDA stream (a cudaStream_t) for callers that order their own work on it. */
+CTLCU_API int ctlcu_stream(ctlcu_ctx* ctx, void** stream);
+
+/* ---- resident volumes --------------------------------------------------------------------- */
+
+/* Upload (data on host) or copy (data_on_device != 0) a float32 volume and
+ * keep it resident in the storage dtype.  Replaces the per-call image upload
+ * of raycasterprojector.cpp:239-269. */
+CTLCU_API int ctlcu_volume_create(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const float* data,
+                        int data_on_device, uint64_t* handle);
+CTLCU_API int ctlcu_volume_release(ctlcu_ctx* ctx, uint64_t handle);
+CTLCU_API int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes);
+
+/* ---- projection -------------------------------------------------------------------------- */
+
+/*
+ * RayCasterProjector::project (raycasterprojector.cpp:139-375) for a resident
+ * volume: all n_views*n_modules matrices in one launch.
+ * pmats and out may each be host or device memory.  With both on the device
+ * the call is asynchronous on `stream` (NULL = the context's stream); with
+ * either on the host the call copies on the context's stream and returns when
+ * `out` is complete.
+ */
+CTLCU_API int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                  const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,
+                  uint32_t rows, float* out, void* stream);
+
+/* One-shot form with the exact argument meaning of RayCasterProjector::project:
+ * the host volume is uploaded for this call only (as the reference does), then
+ * released.  Host or device pmats/out as above; returns when out is complete. */
+CTLCU_API int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const float* volume,
+                         const ctlcu_settings* settings, const double* pmats, uint32_t n_views,
+                         uint32_t n_modules, uint32_t channels, uint32_t rows, float* out);
+
+/*
+ * Batched form: every request's views in one persistent launch (a work list
+ * of (request, view, module, tile) items over all SMs).  Requests may use
+ * different volumes and detector sizes.  All pointers are device memory;
+ * asynchronous on `stream` (NULL = the context's stream).
+ */
+CTLCU_API int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                        const ctlcu_settings* settings, void* stream);
+
+/* Wait for the context's stream; reports a deferred device-side error
+ * (CTLCU_ERR_SINGULAR_GEOMETRY) raised by an earlier asynchronous call. */
+CTLCU_API int ctlcu_sync(ctlcu_ctx* ctx);
+
+/* ---- introspection used by tests and the benchmark ----------------------------------------- */
+
+/* Exact number of volume samples the reference scheme takes for this job
+ * (sum over rays of floor(tmax)+2-floor(tmin)), computed on the device. */
+CTLCU_API int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                        const double* pmats, uint32_t n_views, uint32_t n_modules,
+                        uint32_t channels, uint32_t rows, uint64_t* samples);
+
+/* Per-(view, module) packed QR (15 doubles: Q row-major, R00 R01 R02 R11 R12 R22)
+ * and per-view source position (3 doubles), computed by the device setup
+ * kernel; the reference's decomposeM / determineSource
+ * (raycasterprojector.cpp:527-549).  Host pointers. */
+CTLCU_API int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_views, uint32_t n_modules,
+                     double* qr_out, double* src_out);
+
+/* Number of kernels this library has launched on the context (all calls). */
+CTLCU_API int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

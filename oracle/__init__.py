@@ -1,0 +1,123 @@
+"""Test-only checkers for the CUDA projector.
+
+``project_fp64`` runs the FP64 C restatement (liboracle.so); ``project_ref``
+runs the reference's own kernel and matrix code compiled for the CPU
+(_ref/libctlref.so, built only where the reference sources are present).
+Nothing in the product package imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REF_DIR = "/root/reference"
+
+
+class _Volume(C.Structure):
+    _fields_ = [("n", C.c_longlong * 3), ("voxel_mm", C.c_float * 3), ("offset_mm", C.c_float * 3)]
+
+
+class _Settings(C.Structure):
+    _fields_ = [("rays_per_pixel", C.c_uint * 2), ("ray_sampling", C.c_float),
+                ("volume_upsampling", C.c_uint), ("interpolate", C.c_int)]
+
+
+def build(with_ref: bool | None = None) -> None:
+    """Compile liboracle.so, and _ref/libctlref.so when the reference is present."""
+    subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
+    if with_ref is None:
+        with_ref = os.path.isdir(_REF_DIR)
+    if with_ref:
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={_REF_DIR}"], check=True)
+
+
+_libs: dict = {}
+
+
+def _lib(name: str):
+    if name not in _libs:
+        path = os.path.join(_HERE, name)
+        if not os.path.exists(path):
+            if name == "liboracle.so":
+                build(with_ref=False)
+            else:
+                raise FileNotFoundError(f"{path} is not built (needs the reference sources)")
+        lib = C.CDLL(path)
+        _libs[name] = lib
+    return _libs[name]
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libctlref.so"))
+
+
+def _structs(shape_zyx, voxel_mm, offset_mm, rays, ray_sampling, upsampling, interpolate):
+    vd = _Volume()
+    vd.n[0], vd.n[1], vd.n[2] = int(shape_zyx[2]), int(shape_zyx[1]), int(shape_zyx[0])
+    for k in range(3):
+        vd.voxel_mm[k] = float(voxel_mm[k])
+        vd.offset_mm[k] = float(offset_mm[k])
+    st = _Settings()
+    st.rays_per_pixel[0], st.rays_per_pixel[1] = int(rays[0]), int(rays[1])
+    st.ray_sampling = float(ray_sampling)
+    st.volume_upsampling = int(upsampling)
+    st.interpolate = int(bool(interpolate))
+    return vd, st
+
+
+def _project(which, volume, voxel_mm, pmats, channels, rows, offset_mm=(0, 0, 0), rays=(1, 1),
+             ray_sampling=0.3, upsampling=1, interpolate=True, threads=None):
+    vol = np.ascontiguousarray(volume, dtype=np.float32)
+    P = np.ascontiguousarray(pmats, dtype=np.float64)
+    V, M = P.shape[0], P.shape[1]
+    out = np.zeros((V, M, rows, channels), dtype=np.float32)
+    vd, st = _structs(vol.shape, voxel_mm, offset_mm, rays, ray_sampling, upsampling, interpolate)
+    threads = threads or os.cpu_count() or 1
+    fp = C.POINTER(C.c_float)
+    dp = C.POINTER(C.c_double)
+    if which == "fp64":
+        lib = _lib("liboracle.so")
+        count = C.c_ulonglong(0)
+        rc = lib.oracle_project(vol.ctypes.data_as(fp), C.byref(vd), C.byref(st), P.ctypes.data_as(dp),
+                                C.c_uint(V), C.c_uint(M), C.c_uint(channels), C.c_uint(rows),
+                                out.ctypes.data_as(fp), C.byref(count), C.c_int(threads))
+        if rc:
+            raise ValueError(f"oracle_project failed ({rc})")
+        return out, int(count.value)
+    lib = _lib(os.path.join("_ref", "libctlref.so"))
+    rc = lib.ctlref_project(vol.ctypes.data_as(fp), C.byref(vd), C.byref(st), P.ctypes.data_as(dp),
+                            C.c_uint(V), C.c_uint(M), C.c_uint(channels), C.c_uint(rows),
+                            out.ctypes.data_as(fp), C.c_int(threads))
+    if rc:
+        raise ValueError(f"ctlref_project failed ({rc})")
+    return out
+
+
+def project_fp64(*args, **kw):
+    """FP64 oracle.  Returns (projections [V, M, rows, channels], sample count)."""
+    return _project("fp64", *args, **kw)
+
+
+def project_ref(*args, **kw):
+    """Reference kernel compiled for the CPU.  Returns projections [V, M, rows, channels]."""
+    return _project("ref", *args, **kw)
+
+
+def view_setup(pmats, which="fp64"):
+    """Per (view, module) packed QR (15 doubles) and per-view source positions."""
+    P = np.ascontiguousarray(pmats, dtype=np.float64)
+    V, M = P.shape[0], P.shape[1]
+    qr = np.zeros((V, M, 15))
+    src = np.zeros((V, 3))
+    dp = C.POINTER(C.c_double)
+    if which == "fp64":
+        _lib("liboracle.so").oracle_view_setup(P.ctypes.data_as(dp), C.c_uint(V), C.c_uint(M),
+                                               qr.ctypes.data_as(dp), src.ctypes.data_as(dp))
+    else:
+        _lib(os.path.join("_ref", "libctlref.so")).ctlref_view_setup(
+            P.ctypes.data_as(dp), C.c_uint(V), C.c_uint(M), qr.ctypes.data_as(dp), src.ctypes.data_as(dp))
+    return qr, src

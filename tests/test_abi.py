@@ -1,0 +1,78 @@
+"""The C ABI library: it loads, and exports exactly what include/ctlcu.h declares."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import ctl_b200
+from ctl_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ctlcu.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"CTLCU_API\s+[\w\s\*]+?\b(ctlcu_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    syms = declared_symbols()
+    for name in ("ctlcu_create", "ctlcu_destroy", "ctlcu_volume_create", "ctlcu_volume_release",
+                 "ctlcu_project", "ctlcu_project_volume", "ctlcu_project_batch", "ctlcu_sync",
+                 "ctlcu_last_error"):
+        assert name in syms
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = L.load()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert lib.ctlcu_abi_version() == 1
+
+
+def test_binding_covers_the_header():
+    bound = {name for name, _, _ in L.SIGNATURES}
+    assert bound == set(declared_symbols())
+
+
+def test_only_the_c_abi_is_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    exported = sorted(line.split()[-1] for line in out.splitlines() if " T " in line)
+    assert exported == declared_symbols()
+
+
+def test_struct_layouts_match_the_header():
+    assert ctypes.sizeof(L.VolumeDesc) == 3 * 4 + 3 * 4 + 3 * 4 + 4
+    assert ctypes.sizeof(L.Settings) == 8 * 4
+    assert ctypes.sizeof(L.Request) == 8 + 8 + 8 + 4 * 4
+
+
+def test_default_settings_are_the_reference_defaults():
+    s = L.load().ctlcu_settings_default()
+    assert list(s.rays_per_pixel) == [1, 1]
+    assert abs(s.ray_sampling - 0.3) < 1e-7
+    assert s.volume_upsampling == 1 and s.interpolate == 1
+    assert s.interp_mode == L.INTERP_SOFTWARE and s.accum == L.ACCUM_FP64
+
+
+def test_bad_device_is_rejected_without_compute():
+    lib = L.load()
+    h = ctypes.c_void_p()
+    assert lib.ctlcu_create(1 << 20, ctypes.byref(h)) == L.ERR_NO_DEVICE
+    assert h.value is None
+
+
+def test_null_arguments_are_rejected():
+    lib = L.load()
+    assert lib.ctlcu_create(0, None) == L.ERR_INVALID_ARGUMENT
+    assert lib.ctlcu_destroy(None) == L.ERR_INVALID_ARGUMENT
+    assert lib.ctlcu_sync(None) == L.ERR_INVALID_ARGUMENT
+
+
+def test_package_exports():
+    for name in ("CudaRayCasterProjector", "Context", "Settings", "VoxelVolume"):
+        assert hasattr(ctl_b200, name)

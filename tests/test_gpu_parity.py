@@ -1,0 +1,215 @@
+"""Parity of the CUDA projector (through the C ABI) with the FP64 oracle and
+with the reference's own kernel output.
+
+Tolerance (every case): max over pixels of
+    |gpu - oracle| / max(|oracle|, 1e-3 * max|oracle|)  <=  1e-4
+for FP32 storage with software trilinear interpolation or nearest voxel;
+for BF16/FP16 storage the oracle runs on the dequantised volume.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from ctl_b200 import _lib as L
+from ctl_b200 import geometry as G
+from ctl_b200 import phantom as Ph
+from ctl_b200.projector import Context, Settings, VoxelVolume
+from tests._common import dequant_bf16, dequant_f16, golden_cases, golden_geometry, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _settings(m, **kw):
+    s = Settings(rays_per_pixel=list(m["rays"]), ray_sampling=m["ray_sampling"],
+                 volume_upsampling=m["upsampling"], interpolate=m["interpolate"])
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def _oracle(m, vol, P):
+    out, S = oracle.project_fp64(vol, m["voxel"], P, m["channels"], m["rows"], offset_mm=m["offset"],
+                                 rays=m["rays"], ray_sampling=m["ray_sampling"],
+                                 upsampling=m["upsampling"], interpolate=m["interpolate"])
+    return out, S
+
+
+@pytest.mark.parametrize("case", golden_cases(), ids=lambda c: c[0]["name"])
+def test_golden_cases_match_oracle_and_reference(ctx, case):
+    m, vol, P, ref = case
+    gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
+                             _settings(m))
+    want, _ = _oracle(m, vol, P)
+    e = rel_err(gpu, want)
+    assert e.max() <= TOL, f"max rel err vs FP64 oracle {e.max():.3e}"
+    # against the reference kernel's own output: the FP32-vs-FP64 gap of the reference
+    er = rel_err(gpu, ref)
+    if m["upsampling"] == 0 and m["interpolate"]:
+        assert er.max() < 3e-4
+    elif m["interpolate"]:
+        assert er.max() < 5e-4 and er.mean() < 1e-5
+    else:
+        assert np.quantile(er, 0.999) < 1e-3 and er.mean() < 1e-4
+
+
+@pytest.mark.parametrize("accum,tol", [(L.ACCUM_FP64, TOL), (L.ACCUM_KAHAN, TOL), (L.ACCUM_FP32, 2e-3)])
+def test_accumulation_modes(ctx, accum, tol):
+    m, vol, P, _ = golden_cases()[0]
+    gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
+                             _settings(m, accum=accum))
+    want, _ = _oracle(m, vol, P)
+    assert rel_err(gpu, want).max() <= tol
+
+
+@pytest.mark.parametrize("storage,deq", [(L.BF16, dequant_bf16), (L.F16, dequant_f16)])
+def test_reduced_precision_storage_vs_dequantised_oracle(ctx, storage, deq):
+    m, vol, P, _ = golden_cases()[0]
+    for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
+        gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
+                                 _settings(m, storage=storage, accum=accum))
+        want, _ = _oracle(m, deq(vol), P)
+        assert rel_err(gpu, want).max() <= TOL
+
+
+def test_texture_filter_is_close_but_coarser(ctx):
+    """Hardware filtering uses 8-bit fractional weights: close, not 1e-4."""
+    m, vol, P, _ = golden_cases()[0]
+    gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
+                             _settings(m, interp_mode=L.INTERP_TEXTURE))
+    want, _ = _oracle(m, vol, P)
+    e = rel_err(gpu, want)
+    assert e.max() < 2e-2 and e.mean() < 2e-3
+
+
+def test_view_setup_matches_reference_mat_code(ctx):
+    g = golden_geometry()
+    for key in ("tube", "carm"):
+        qr, src = ctx.view_setup(g[f"{key}_pmats"])
+        np.testing.assert_allclose(qr, g[f"{key}_qr"], rtol=0, atol=1e-9 * np.abs(g[f"{key}_qr"]).max())
+        np.testing.assert_allclose(src, g[f"{key}_src"], rtol=0, atol=1e-9)
+
+
+def test_sample_count_matches_oracle(ctx):
+    for m, vol, P, _ in golden_cases():
+        v = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]))
+        n = ctx.count_samples(v, P, m["channels"], m["rows"], _settings(m))
+        _, S = _oracle(m, vol, P)
+        assert abs(n - S) <= max(2, 1e-5 * S), (m["name"], n, S)
+        v.release()
+
+
+def test_resident_device_and_host_paths_agree_bitwise(ctx):
+    import torch
+    m, vol, P, _ = golden_cases()[5]
+    s = _settings(m)
+    host = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"], s)
+    v = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]))
+    res = ctx.project(v, P, m["channels"], m["rows"], s)
+    dP = torch.from_numpy(np.ascontiguousarray(P)).cuda()
+    dev = ctx.project(v, dP, m["channels"], m["rows"], s)
+    ctx.sync()
+    np.testing.assert_array_equal(host, res)
+    np.testing.assert_array_equal(host, dev.cpu().numpy())
+    v.release()
+
+
+def test_batch_equals_individual_calls(ctx):
+    import torch
+    cases = golden_cases()
+    reqs, singles = [], []
+    vols = []
+    for m, vol, P, _ in (cases[0], cases[5], cases[7]):
+        v = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]))
+        vols.append(v)
+        dP = torch.from_numpy(np.ascontiguousarray(P)).cuda()
+        out = torch.zeros((P.shape[0], P.shape[1], m["rows"], m["channels"]), device="cuda")
+        reqs.append((v, dP, out))
+        singles.append(ctx.project(v, P, m["channels"], m["rows"], Settings()))
+    ctx.project_batch(reqs, Settings())
+    ctx.sync()
+    for (v, dP, out), want in zip(reqs, singles):
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+    for v in vols:
+        v.release()
+
+
+def test_errors_are_status_codes(ctx):
+    m, vol, P, _ = golden_cases()[0]
+    with pytest.raises(L.CtlcuError) as e:
+        ctx.project(type("V", (), {"handle": 987654})(), P, 8, 8)
+    assert e.value.status == L.ERR_INVALID_HANDLE
+    with pytest.raises(L.CtlcuError) as e:
+        ctx.project_volume(VoxelVolume(vol, m["voxel"]), P, 8, 8, Settings(ray_sampling=0.0))
+    assert e.value.status == L.ERR_INVALID_ARGUMENT
+    with pytest.raises(L.CtlcuError) as e:
+        ctx.project_volume(VoxelVolume(vol, (0.0, 1.0, 1.0)), P, 8, 8)
+    assert e.value.status == L.ERR_INVALID_ARGUMENT
+    # a singular matrix: status code, its pixels are zero, the others are projected
+    Pbad = P[:2].copy()
+    Pbad[1, 0, :, :3] = 0.0
+    with pytest.raises(L.CtlcuError) as e:
+        ctx.project_volume(VoxelVolume(vol, m["voxel"]), Pbad, 16, 16)
+    assert e.value.status == L.ERR_SINGULAR_GEOMETRY
+    ctx.sync()
+    # memory budget: admission refused, nothing leaked
+    used = ctx.memory_used()
+    ctx.set_memory_budget(used + 1024)
+    with pytest.raises(L.CtlcuError) as e:
+        ctx.volume(VoxelVolume(vol, m["voxel"]))
+    assert e.value.status == L.ERR_OUT_OF_MEMORY
+    ctx.set_memory_budget(0)
+    assert ctx.memory_used() == used
+
+
+# ---- full-size configurations, checked with the oracle on a few views -------------------------
+
+def _c2_geometry(n_views=360):
+    det = G.FlatDetector(512, 512, 0.6, 0.6)
+    fan = G.fan_angle(det, 1200.0)
+    return G.circular_flat(n_views, 750.0, 1200.0, det, angle_range=np.pi * 200 / 180 + fan,
+                           rng=np.random.default_rng(2024), jitter_mm=0.5, tilt_deg=0.2)
+
+
+def test_c2_full_size_views_match_oracle(ctx):
+    """256^3 -> 512^2: two full views of the short-scan configuration against the oracle."""
+    vol = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=2)
+    P = _c2_geometry()[[0, 181]]
+    v = ctx.volume(VoxelVolume(vol, (1, 1, 1)))
+    for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
+        gpu = ctx.project(v, P, 512, 512, Settings(accum=accum))
+        want, _ = oracle.project_fp64(vol, (1, 1, 1), P, 512, 512)
+        e = rel_err(gpu, want)
+        assert e.max() <= TOL, e.max()
+    v.release()
+
+
+def test_c2_linearity_at_full_size(ctx):
+    """project(2 a + b) = 2 project(a) + project(b) over all 360 views (size-independent check)."""
+    a = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=2)
+    b = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=3)
+    P = _c2_geometry()
+    pa = ctx.project_volume(VoxelVolume(a, (1, 1, 1)), P, 512, 512)
+    pb = ctx.project_volume(VoxelVolume(b, (1, 1, 1)), P, 512, 512)
+    pc = ctx.project_volume(VoxelVolume(2 * a + b, (1, 1, 1)), P, 512, 512)
+    e = rel_err(pc, 2 * pa + pb)
+    assert e.max() < 1e-5
+
+
+def test_uniform_cube_chord_full_detector(ctx):
+    """A uniform 128^3 cube: every central-row pixel's value is mu times its chord (+- one step)."""
+    n, mu = 128, 0.02
+    vol = np.full((n, n, n), mu, np.float32)
+    det = G.FlatDetector(257, 257, 1.0, 1.0)
+    P = G.circular_flat(1, 750.0, 1000.0, det)
+    out = ctx.project_volume(VoxelVolume(vol, (1, 1, 1)), P, 257, 257)
+    assert abs(out[0, 0, 128, 128] - mu * n) <= 2 * mu * 0.3
+    assert out[0, 0, 0, 0] == 0.0
