@@ -49,7 +49,9 @@ METRIC = "projections/s at 256^3->512^2 (plain FP32)"
 WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
 
 
-def make_inputs():
+def make_inputs(n_views: int = N_VIEWS):
+    """The phantom and the 360-view geometry; n_views < 360 takes evenly spaced views
+    of the same scan (a small case for profiling)."""
     from ctl_b200 import geometry as G
     from ctl_b200 import phantom as Ph
     vol = Ph.ellipsoid_phantom(SHAPE, VOXEL, 40, seed=2)
@@ -57,6 +59,8 @@ def make_inputs():
     fan = G.fan_angle(det, 1200.0)
     P = G.circular_flat(N_VIEWS, 750.0, 1200.0, det, angle_range=math.radians(200.0) + fan,
                         rng=np.random.default_rng(2024), jitter_mm=0.5, tilt_deg=0.2)
+    if n_views < N_VIEWS:
+        P = np.ascontiguousarray(P[np.linspace(0, N_VIEWS - 1, n_views).round().astype(int)])
     return vol, P
 
 
@@ -202,15 +206,18 @@ def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    vol, P = make_inputs()
+    n_views = args.views
+    vol, P = make_inputs(n_views)
     settings = Settings(accum={"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[args.accum],
-                        storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage])
+                        storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage],
+                        interp_mode=L.INTERP_TEXTURE if args.interp == "texture" else L.INTERP_SOFTWARE,
+                        kernel={"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS}[args.kernel])
     ctx = Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     vobj = VoxelVolume(vol, VOXEL)
     volume = ctx.volume(vobj, settings.storage)
     dP = torch.from_numpy(P).to(dev)
-    out = torch.empty((N_VIEWS, 1, ROWS, CHANNELS), dtype=torch.float32, device=dev)
+    out = torch.empty((n_views, 1, ROWS, CHANNELS), dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     samples = ctx.count_samples(volume, P, CHANNELS, ROWS, settings)
 
@@ -238,7 +245,7 @@ def run_ours(args):
         step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
     ms_per_step = total_ms / args.steps
-    value = world * N_VIEWS * args.steps / (total_ms / 1e3)
+    value = world * n_views * args.steps / (total_ms / 1e3)
 
     # the projection kernel alone: each step is one setup launch + one projection launch;
     # time a setup-only run to split them
@@ -248,7 +255,7 @@ def run_ours(args):
     # e2e through the C ABI with host buffers (pinned)
     h_vol = torch.from_numpy(vol).pin_memory()
     h_P = torch.from_numpy(P).pin_memory()
-    h_out = torch.empty((N_VIEWS, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
+    h_out = torch.empty((n_views, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
     desc_vol = VoxelVolume(h_vol.numpy(), VOXEL)
     for _ in range(max(1, args.warmup // 2)):
         ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
@@ -260,12 +267,12 @@ def run_ours(args):
         ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = max_over_ranks(sum(e2e_ms), world)
-    e2e_value = world * N_VIEWS * len(e2e_ms) / (e2e_total / 1e3)
+    e2e_value = world * n_views * len(e2e_ms) / (e2e_total / 1e3)
     clk = clocks.stop()
 
     if rank == 0:
         b = 4 if settings.storage == L.F32 else 2
-        alg_bytes = samples * 8 * b + 4 * N_VIEWS * ROWS * CHANNELS
+        alg_bytes = samples * 8 * b + 4 * n_views * ROWS * CHANNELS
         props = torch.cuda.get_device_properties(dev)
         sms = props.multi_processor_count
         mhz = clk.get("sm_mhz") or 1965.0
@@ -278,7 +285,8 @@ def run_ours(args):
             "dtype": {L.F32: "f32", L.BF16: "bf16", L.F16: "f16"}[settings.storage] + "-storage/f32-interp/"
                      + args.accum + "-accum",
             "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
-            "config": {"workload": WORKLOAD, "views_per_step": N_VIEWS, "volume": "256^3", "detector": "512x512",
+            "config": {"workload": WORKLOAD, "views_per_step": n_views, "volume": "256^3", "detector": "512x512",
+                       "interp": args.interp, "kernel": args.kernel,
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"views replicated per GPU x{world}"},
             "samples_per_step": samples,
@@ -318,6 +326,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--accum", choices=["fp64", "kahan", "fp32"], default="fp64")
     ap.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32")
+    ap.add_argument("--interp", choices=["software", "texture"], default="software")
+    ap.add_argument("--kernel", choices=["auto", "gather", "cells"], default="auto")
+    ap.add_argument("--views", type=int, default=N_VIEWS,
+                    help="views per step (360 = the configuration; fewer = a small profiling case)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)

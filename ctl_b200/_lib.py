@@ -24,6 +24,7 @@ ERR_BUSY = 8
 F32, BF16, F16 = 0, 1, 2
 INTERP_SOFTWARE, INTERP_TEXTURE = 0, 1
 ACCUM_FP64, ACCUM_KAHAN, ACCUM_FP32 = 0, 1, 2
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS = 0, 1, 2
 
 STATUS_NAMES = {
     OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",
@@ -40,7 +41,7 @@ class VolumeDesc(C.Structure):
 class Settings(C.Structure):
     _fields_ = [("rays_per_pixel", C.c_uint32 * 2), ("ray_sampling", C.c_float),
                 ("volume_upsampling", C.c_uint32), ("interpolate", C.c_int32),
-                ("interp_mode", C.c_int32), ("accum", C.c_int32), ("reserved", C.c_int32)]
+                ("interp_mode", C.c_int32), ("accum", C.c_int32), ("kernel", C.c_int32)]
 
 
 class Request(C.Structure):

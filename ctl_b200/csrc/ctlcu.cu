@@ -35,6 +35,8 @@ struct VolumeEntry {
     size_t bytes = 0;
     bool pooled = false;
     float* mean = nullptr;      // padded 1x1x1 mean volume (f = 0), float
+    void* cells = nullptr;      // coefficient cells (CTLCU_KERNEL_CELLS), built on first use
+    size_t cell_bytes = 0;
     std::map<int, TexEntry> tex;  // hardware-filter copies keyed by up-sampling factor
 };
 
@@ -110,8 +112,12 @@ int check_settings(ctlcu_ctx* ctx, const ctlcu_settings* s)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown interp_mode %d", s->interp_mode);
     if (s->accum < CTLCU_ACCUM_FP64 || s->accum > CTLCU_ACCUM_FP32)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown accum %d", s->accum);
-    if (s->reserved != 0)
-        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "reserved must be 0");
+    if (s->kernel < CTLCU_KERNEL_AUTO || s->kernel > CTLCU_KERNEL_CELLS)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown kernel %d", s->kernel);
+    if (s->kernel == CTLCU_KERNEL_CELLS &&
+        (!s->interpolate || s->interp_mode != CTLCU_INTERP_SOFTWARE || s->volume_upsampling != 1))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "the cell kernel needs software trilinear interpolation and volumeUpSampling 1");
     return CTLCU_OK;
 }
 
@@ -196,6 +202,15 @@ void free_volume(ctlcu_ctx* ctx, VolumeEntry& v)
     if (v.mean)
         cudaFreeAsync(v.mean, ctx->stream);
     v.mean = nullptr;
+    if (v.cells) {
+        if (v.pooled)
+            cudaFreeAsync(v.cells, ctx->stream);
+        else
+            cudaFree(v.cells);
+        ctx->used -= std::min<uint64_t>(ctx->used, v.cell_bytes);
+    }
+    v.cells = nullptr;
+    v.cell_bytes = 0;
     if (v.data) {
         if (v.pooled)
             cudaFreeAsync(v.data, ctx->stream);
@@ -222,6 +237,30 @@ int ensure_mean(ctlcu_ctx* ctx, VolumeEntry& v)
     CU_TRY(ctx, launch_mean_volume(sum, (double)n[0] * n[1] * n[2], v.mean, ctx->stream));
     ctx->launches += 2;
     CU_TRY(ctx, cudaFreeAsync(sum, ctx->stream));
+    return CTLCU_OK;
+}
+
+// Coefficient cells of the padded volume, built once per volume on its first
+// cell-kernel projection.
+int ensure_cells(ctlcu_ctx* ctx, VolumeEntry& v)
+{
+    if (v.cells)
+        return CTLCU_OK;
+    const int n[3] = { (int)v.desc.n[0], (int)v.desc.n[1], (int)v.desc.n[2] };
+    const size_t ncell = (size_t)(n[0] + 2 * kPad - 1) * (n[1] + 2 * kPad - 1) * (n[2] + 2 * kPad - 1);
+    const size_t bytes = ncell * kCellBytes;
+    if (ctx->budget && ctx->used + bytes > ctx->budget)
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY,
+                    "cell array of %zu bytes exceeds the memory budget (%llu of %llu bytes used)", bytes,
+                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    if (v.pooled)
+        CU_TRY(ctx, cudaMallocAsync(&v.cells, bytes, ctx->stream));
+    else
+        CU_TRY(ctx, cudaMalloc(&v.cells, bytes));
+    v.cell_bytes = bytes;
+    ctx->used += bytes;
+    CU_TRY(ctx, launch_build_cells(v.data, n, v.desc.dtype, v.cells, ctx->stream));
+    ++ctx->launches;
     return CTLCU_OK;
 }
 
@@ -328,6 +367,18 @@ int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, Project
         if (r)
             return r;
     }
+    if (mode == Mode::Trilinear && f == 1 && s->kernel != CTLCU_KERNEL_GATHER) {
+        int r = ensure_cells(ctx, v);
+        if (r)
+            return r;
+        mode = Mode::Cells;
+        a.cells = v.cells;
+        const uint32_t cx = a.ext[0] - 1, cy = a.ext[1] - 1, cz = a.ext[2] - 1;
+        a.csy = cx;
+        a.csz = cx * cy;
+        a.cmax = cx * cy * cz - 1;
+        a.ckoff = kMagicBits * (1u + a.csy + a.csz);  // mod 2^32
+    }
     a.sy = a.ext[0];
     a.sz = a.ext[0] * a.ext[1];
     const float smallest = std::min(std::min(voxel[0], voxel[1]), voxel[2]);
@@ -349,6 +400,7 @@ void job_args(ProjectArgs& a, const ctlcu_settings* s, uint32_t V, uint32_t M, u
     a.tiles_per_vm = a.tiles_x * ((R + kTileY - 1) / kTileY);
     a.rays_x = s->rays_per_pixel[0];
     a.rays_y = s->rays_per_pixel[1];
+    a.vm_group = 8;
 }
 
 VolumeEntry* find_volume(ctlcu_ctx* ctx, uint64_t h)
@@ -450,7 +502,7 @@ ctlcu_settings ctlcu_settings_default(void)
     s.interpolate = 1;
     s.interp_mode = CTLCU_INTERP_SOFTWARE;
     s.accum = CTLCU_ACCUM_FP64;
-    s.reserved = 0;
+    s.kernel = CTLCU_KERNEL_AUTO;
     return s;
 }
 
@@ -595,7 +647,7 @@ int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes)
     VolumeEntry* v = find_volume(ctx, handle);
     if (!v)
         return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)handle);
-    uint64_t b = v->bytes;
+    uint64_t b = v->bytes + v->cell_bytes;
     for (auto& t : v->tex)
         b += t.second.bytes;
     *bytes = b;

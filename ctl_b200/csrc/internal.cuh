@@ -34,7 +34,15 @@ struct ViewGeom {
     int pad_;
 };
 
-enum class Mode : int { Trilinear = 0, Nearest = 1, Texture = 2 };
+// Round-to-integer constant: for |v| < 2^22, the float sum v + kMagic is
+// kMagic + rint(v) and its bit pattern is kMagicBits + rint(v).
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr uint32_t kMagicBits = 0x4B400000u;
+
+// Bytes per cell of the coefficient cell array (8 floats).
+constexpr int kCellBytes = 32;
+
+enum class Mode : int { Trilinear = 0, Nearest = 1, Texture = 2, Cells = 3 };
 enum class Accum : int { F64 = 0, Kahan = 1, F32 = 2 };
 
 // Everything a projection launch needs, passed by value.
@@ -48,6 +56,11 @@ struct ProjectArgs {
     double voxel[3];          // voxel size of that grid (mm)
     double corner[3];         // low corner of that grid (mm)
     double increment;         // step length (mm)
+    const void* cells;        // Mode::Cells: coefficient cells, x fastest
+    uint32_t csy, csz;        // cell strides (cells per row, per slice)
+    uint32_t cmax;            // last valid cell index
+    uint32_t ckoff;           // kMagicBits * (1 + csy + csz) mod 2^32
+    uint32_t vm_group;        // blocks cover `vm_group` consecutive view-modules per tile
     const ViewGeom* geom;     // [n_vm]
     float* out;               // [n_vm][rows][channels]
     uint32_t channels, rows;
@@ -67,6 +80,7 @@ cudaError_t launch_count(const ProjectArgs& a, Mode mode, cudaStream_t s);
 cudaError_t launch_pad_convert(const float* src, void* dst, const int n[3], int dtype, cudaStream_t s);
 cudaError_t launch_mean(const void* padded, const int n[3], int dtype, double* sum_out, cudaStream_t s);
 cudaError_t launch_mean_volume(const double* sum, double count, float* dst_padded, cudaStream_t s);
+cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, void* cells, cudaStream_t s);
 cudaError_t launch_unpad_upsample(const void* padded, const int n[3], int dtype, int f, void* dst,
                                   cudaStream_t s);
 

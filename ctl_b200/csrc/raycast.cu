@@ -143,6 +143,22 @@ __device__ __forceinline__ Ray setup_ray(const ProjectArgs& a, const ViewGeom& g
         r.step[0] = r.step[1] = r.step[2] = 0.0;
         return r;
     }
+    if (M == Mode::Cells) {
+        // Only samples inside the box contribute (the reference's first and last
+        // samples, floor(tmin) and floor(tmax)+1, lie outside it and read zeros),
+        // so the loop runs over ceil(t0) .. floor(t1).  Coordinates are
+        // v = p - 1 + pad: the cell index is rint(v), the offset from the
+        // cell centre v - rint(v).
+        const double i0 = ceil(t0), i1 = floor(t1);
+        r.n = i1 >= i0 ? static_cast<int>(i1 - i0) + 1 : 0;
+        r.base[0] = (s0 - k0) + i0 * d0 + (kPad - 1.0);
+        r.base[1] = (s1 - k1) + i0 * d1 + (kPad - 1.0);
+        r.base[2] = (s2 - k2) + i0 * d2 + (kPad - 1.0);
+        r.step[0] = d0;
+        r.step[1] = d1;
+        r.step[2] = d2;
+        return r;
+    }
     const double i0 = floor(t0), i1 = floor(t1) + 1.0;
     r.n = static_cast<int>(i1 - i0) + 1;
     // position relative to the corner: (source - corner) + i * step
@@ -245,6 +261,73 @@ __device__ __forceinline__ void march_nearest(const ProjectArgs& a, const Ray& r
     }
 }
 
+// One sample from the coefficient cells at step kk (both lanes of kk hold k).
+// Per axis: v = base + k step; t = v + kMagic rounds v to the cell index
+// (its bits minus kMagicBits); h = v - (t - kMagic) is the offset from the
+// cell centre in [-1/2, 1/2].  x and y go through packed f32x2 arithmetic.
+// A sample that lands exactly between two cells may take either of them; both
+// give the same interpolated value.  The cell index is clamped to the array as
+// a guard; the loop bounds already keep every sample inside it.
+__device__ __forceinline__ float cell_sample(const char* __restrict__ cells, float2 kk, float2 bxy,
+                                             float bz, float2 dxy, float dz, uint32_t sy, uint32_t sz,
+                                             uint32_t koff, uint32_t cmax)
+{
+    const float2 magic2 = make_float2(kMagic, kMagic);
+    const float2 nmagic2 = make_float2(-kMagic, -kMagic);
+    const float2 none2 = make_float2(-1.0f, -1.0f);
+    const float2 vxy = __ffma2_rn(kk, dxy, bxy);
+    const float vz = fmaf(kk.x, dz, bz);
+    const float2 txy = __fadd2_rn(vxy, magic2);
+    const float tz = __fadd_rn(vz, kMagic);
+    const float2 fxy = __fadd2_rn(txy, nmagic2);
+    const float fz = __fadd_rn(tz, -kMagic);
+    const float2 hxy = __ffma2_rn(fxy, none2, vxy);
+    const float hz = fmaf(fz, -1.0f, vz);
+    uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz - koff;
+    idx = min(idx, cmax);
+    const char* p = cells + (size_t)idx * kCellBytes;
+    float c0, c1, c2, c3, c4, c5, c6, c7;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(c0), "=f"(c1), "=f"(c2), "=f"(c3), "=f"(c4), "=f"(c5), "=f"(c6), "=f"(c7)
+        : "l"(p));
+    // (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
+    const float2 hx2 = make_float2(hxy.x, hxy.x);
+    const float2 ea = __ffma2_rn(hx2, make_float2(c2, c3), make_float2(c0, c1));
+    const float2 eb = __ffma2_rn(hx2, make_float2(c6, c7), make_float2(c4, c5));
+    const float2 g = __ffma2_rn(make_float2(hxy.y, hxy.y), eb, ea);
+    return fmaf(hz, g.y, g.x);
+}
+
+// Sample loop over the coefficient cells, four samples per partial sum.
+template <Accum ACC>
+__device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
+{
+    const char* __restrict__ cells = static_cast<const char*>(a.cells);
+    const float2 bxy = make_float2((float)r.base[0], (float)r.base[1]);
+    const float bz = (float)r.base[2];
+    const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
+    const float dz = (float)r.step[2];
+    const uint32_t sy = a.csy, sz = a.csz, koff = a.ckoff, cmax = a.cmax;
+    const float2 one2 = make_float2(1.0f, 1.0f);
+    float2 kk = make_float2(0.0f, 0.0f);
+    int k = 0;
+    for (; k + 4 <= r.n; k += 4) {
+        float part = cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
+        kk = __fadd2_rn(kk, one2);
+        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
+        kk = __fadd2_rn(kk, one2);
+        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
+        kk = __fadd2_rn(kk, one2);
+        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
+        kk = __fadd2_rn(kk, one2);
+        acc.add(part);
+    }
+    for (; k < r.n; ++k) {
+        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax));
+        kk = __fadd2_rn(kk, one2);
+    }
+}
+
 // Sample loop, hardware texture filter (border colour 0, unnormalised coords).
 template <Accum ACC>
 __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
@@ -259,9 +342,18 @@ __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r
 
 __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
 {
+    // Blocks run in order (group of vm_group view-modules, tile, view-module in
+    // group): blocks resident at the same time cover one detector tile of
+    // neighbouring views, whose rays cross nearly the same part of the volume.
     const uint32_t b = blockIdx.x;
-    vm = b / a.tiles_per_vm;
-    const uint32_t t = b - vm * a.tiles_per_vm;
+    const uint32_t G = a.vm_group;
+    const uint32_t per_group = G * a.tiles_per_vm;
+    const uint32_t g = b / per_group;
+    const uint32_t first = g * G;
+    const uint32_t gsize = min(G, a.n_vm - first);
+    const uint32_t r = b - g * per_group;
+    const uint32_t t = r / gsize;
+    vm = first + (r - t * gsize);
     const uint32_t ty = t / a.tiles_x, tx = t - ty * a.tiles_x;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     x = tx * kTileX + (warp & 1u) * 8u + (lane & 7u);
@@ -288,7 +380,9 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjectArgs a)
             const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
             const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
             const Ray r = setup_ray<M>(a, g, px, py, a.flags);
-            if (M == Mode::Trilinear)
+            if (M == Mode::Cells)
+                march_cells<ACC>(a, r, acc);
+            else if (M == Mode::Trilinear)
                 march_trilinear<T, ACC, UP>(a, r, acc);
             else if (M == Mode::Nearest)
                 march_nearest<T, ACC>(a, r, acc);
@@ -336,8 +430,8 @@ cudaError_t launch_typed(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_
 template <Mode M, Accum ACC>
 cudaError_t launch_mode(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
 {
-    if (M == Mode::Texture) {
-        project_kernel<float, Mode::Texture, ACC, false><<<grid, kBlock, 0, s>>>(a);
+    if (M == Mode::Texture || M == Mode::Cells) {
+        project_kernel<float, M, ACC, false><<<grid, kBlock, 0, s>>>(a);
         return cudaGetLastError();
     }
     if (M == Mode::Trilinear && a.up != 1)
@@ -352,6 +446,7 @@ cudaError_t launch_acc(const ProjectArgs& a, Mode mode, int dtype, dim3 grid, cu
     case Mode::Trilinear: return launch_mode<Mode::Trilinear, ACC>(a, dtype, grid, s);
     case Mode::Nearest: return launch_mode<Mode::Nearest, ACC>(a, dtype, grid, s);
     case Mode::Texture: return launch_mode<Mode::Texture, ACC>(a, dtype, grid, s);
+    case Mode::Cells: return launch_mode<Mode::Cells, ACC>(a, dtype, grid, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -104,6 +104,54 @@ __global__ void upsample_kernel(const T* __restrict__ padded, int nx, int ny, in
     }
 }
 
+// Coefficient cells.  Cell (i, j, k) spans padded voxels i..i+1, j..j+1, k..k+1.
+// With h = w - 1/2 the local offsets from the cell centre, its trilinear
+// interpolant is
+//   f = C0 + Cx hx + Cy hy + Cz hz + Cxy hx hy + Cxz hx hz + Cyz hy hz + Cxyz hx hy hz,
+//   C0 = sum v / 8, Cx = sum sx v / 4, Cxy = sum sx sy v / 2, Cxyz = sum sx sy sz v
+// (s = -1 for the low corner, +1 for the high one, per axis).  The 8
+// coefficients are computed in FP64 and stored as FP32 in the order
+//   (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
+// so the sampler evaluates f with three packed f32x2 FMAs and one FMA.
+template <typename T>
+__global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey, int ez,
+                                   float4* __restrict__ cells)
+{
+    const int cx = ex - 1, cy = ey - 1, cz = ez - 1;
+    const size_t total = (size_t)cx * cy * cz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % cx);
+        const size_t r = i / cx;
+        const int y = (int)(r % cy);
+        const int z = (int)(r / cy);
+        const size_t o = (size_t)x + (size_t)ex * ((size_t)y + (size_t)ey * z);
+        const size_t sy = ex, sz = (size_t)ex * ey;
+        double v[2][2][2];  // [z][y][x]
+        for (int c = 0; c < 2; ++c)
+            for (int b = 0; b < 2; ++b)
+                for (int a = 0; a < 2; ++a)
+                    v[c][b][a] = (double)to_float<T>(padded[o + a + b * sy + c * sz]);
+        double C0 = 0, Cx = 0, Cy = 0, Cz = 0, Cxy = 0, Cxz = 0, Cyz = 0, Cxyz = 0;
+        for (int c = 0; c < 2; ++c)
+            for (int b = 0; b < 2; ++b)
+                for (int a = 0; a < 2; ++a) {
+                    const double sx = a ? 1.0 : -1.0, sy_ = b ? 1.0 : -1.0, sz_ = c ? 1.0 : -1.0;
+                    const double t = v[c][b][a];
+                    C0 += t;
+                    Cx += sx * t;
+                    Cy += sy_ * t;
+                    Cz += sz_ * t;
+                    Cxy += sx * sy_ * t;
+                    Cxz += sx * sz_ * t;
+                    Cyz += sy_ * sz_ * t;
+                    Cxyz += sx * sy_ * sz_ * t;
+                }
+        cells[2 * i] = make_float4((float)(C0 * 0.125), (float)(Cz * 0.25), (float)(Cx * 0.25), (float)(Cxz * 0.5));
+        cells[2 * i + 1] = make_float4((float)(Cy * 0.25), (float)(Cyz * 0.5), (float)(Cxy * 0.5), (float)Cxyz);
+    }
+}
+
 unsigned grid_for(size_t n)
 {
     size_t b = (n + 255) / 256;
@@ -141,6 +189,19 @@ cudaError_t launch_mean(const void* padded, const int n[3], int dtype, double* s
 cudaError_t launch_mean_volume(const double* sum, double count, float* dst_padded, cudaStream_t s)
 {
     mean_volume_kernel<<<1, 1, 0, s>>>(sum, count, dst_padded);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, void* cells, cudaStream_t s)
+{
+    const int ex = n[0] + 2 * kPad, ey = n[1] + 2 * kPad, ez = n[2] + 2 * kPad;
+    const unsigned g = grid_for((size_t)(ex - 1) * (ey - 1) * (ez - 1));
+    switch (dtype) {
+    case 0: build_cells_kernel<float><<<g, 256, 0, s>>>((const float*)padded, ex, ey, ez, (float4*)cells); break;
+    case 1: build_cells_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16*)padded, ex, ey, ez, (float4*)cells); break;
+    case 2: build_cells_kernel<__half><<<g, 256, 0, s>>>((const __half*)padded, ex, ey, ez, (float4*)cells); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

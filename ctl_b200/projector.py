@@ -79,6 +79,7 @@ class Settings:
     interp_mode: int = L.INTERP_SOFTWARE
     accum: int = L.ACCUM_FP64
     storage: int = L.F32
+    kernel: int = L.KERNEL_AUTO
 
     def to_c(self) -> L.Settings:
         s = L.Settings()
@@ -89,7 +90,7 @@ class Settings:
         s.interpolate = 1 if self.interpolate else 0
         s.interp_mode = int(self.interp_mode)
         s.accum = int(self.accum)
-        s.reserved = 0
+        s.kernel = int(self.kernel)
         return s
 
     @staticmethod

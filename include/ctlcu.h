@@ -63,6 +63,17 @@ typedef enum {
     CTLCU_ACCUM_FP32 = 2   /* plain float */
 } ctlcu_accum;
 
+/*
+ * Sample-loop variant.  AUTO picks CELLS for software trilinear interpolation
+ * without up-sampling and GATHER otherwise.
+ *   GATHER  eight scalar loads per sample from the zero-padded voxel array
+ *   CELLS   one 32-byte load per sample from a derived cell array holding,
+ *           per trilinear cell, the 8 coefficients of its interpolation
+ *           polynomial about the cell centre (FP32, built on the device once
+ *           per resident volume; 8x the voxel count x 4 bytes)
+ */
+typedef enum { CTLCU_KERNEL_AUTO = 0, CTLCU_KERNEL_GATHER = 1, CTLCU_KERNEL_CELLS = 2 } ctlcu_kernel;
+
 typedef struct ctlcu_ctx ctlcu_ctx;
 
 typedef struct {
@@ -76,7 +87,7 @@ typedef struct {
  * RayCasterProjector::Settings (raycasterprojector.h:27-37) plus the
  * B200 options.  ctlcu_settings_default() gives the reference defaults:
  * rays {1,1}, raySampling 0.3, volumeUpSampling 1, interpolate on,
- * software interpolation, FP64 accumulation.
+ * software interpolation, FP64 accumulation, automatic kernel choice.
  */
 typedef struct {
     uint32_t rays_per_pixel[2]; /* sub-rays along channel (x) and row (y), 1..64 */
@@ -85,7 +96,7 @@ typedef struct {
     int32_t interpolate;        /* 1 trilinear, 0 nearest voxel (forces up-sampling 1) */
     int32_t interp_mode;        /* ctlcu_interp_mode */
     int32_t accum;              /* ctlcu_accum */
-    int32_t reserved;           /* must be 0 */
+    int32_t kernel;             /* ctlcu_kernel: sample-loop variant (0 = automatic) */
 } ctlcu_settings;
 
 /* One projection request of a batch: device pointers, see ctlcu_project_batch. */

@@ -43,11 +43,12 @@ def _oracle(m, vol, P):
     return out, S
 
 
+@pytest.mark.parametrize("kernel", [L.KERNEL_AUTO, L.KERNEL_GATHER], ids=["auto", "gather"])
 @pytest.mark.parametrize("case", golden_cases(), ids=lambda c: c[0]["name"])
-def test_golden_cases_match_oracle_and_reference(ctx, case):
+def test_golden_cases_match_oracle_and_reference(ctx, case, kernel):
     m, vol, P, ref = case
     gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
-                             _settings(m))
+                             _settings(m, kernel=kernel))
     want, _ = _oracle(m, vol, P)
     e = rel_err(gpu, want)
     assert e.max() <= TOL, f"max rel err vs FP64 oracle {e.max():.3e}"
@@ -61,21 +62,23 @@ def test_golden_cases_match_oracle_and_reference(ctx, case):
         assert np.quantile(er, 0.999) < 1e-3 and er.mean() < 1e-4
 
 
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER], ids=["cells", "gather"])
 @pytest.mark.parametrize("accum,tol", [(L.ACCUM_FP64, TOL), (L.ACCUM_KAHAN, TOL), (L.ACCUM_FP32, 2e-3)])
-def test_accumulation_modes(ctx, accum, tol):
+def test_accumulation_modes(ctx, accum, tol, kernel):
     m, vol, P, _ = golden_cases()[0]
     gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
-                             _settings(m, accum=accum))
+                             _settings(m, accum=accum, kernel=kernel))
     want, _ = _oracle(m, vol, P)
     assert rel_err(gpu, want).max() <= tol
 
 
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER], ids=["cells", "gather"])
 @pytest.mark.parametrize("storage,deq", [(L.BF16, dequant_bf16), (L.F16, dequant_f16)])
-def test_reduced_precision_storage_vs_dequantised_oracle(ctx, storage, deq):
+def test_reduced_precision_storage_vs_dequantised_oracle(ctx, storage, deq, kernel):
     m, vol, P, _ = golden_cases()[0]
     for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
         gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
-                                 _settings(m, storage=storage, accum=accum))
+                                 _settings(m, storage=storage, accum=accum, kernel=kernel))
         want, _ = _oracle(m, deq(vol), P)
         assert rel_err(gpu, want).max() <= TOL
 
@@ -184,12 +187,21 @@ def test_c2_full_size_views_match_oracle(ctx):
     vol = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=2)
     P = _c2_geometry()[[0, 181]]
     v = ctx.volume(VoxelVolume(vol, (1, 1, 1)))
-    for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
-        gpu = ctx.project(v, P, 512, 512, Settings(accum=accum))
-        want, _ = oracle.project_fp64(vol, (1, 1, 1), P, 512, 512)
-        e = rel_err(gpu, want)
-        assert e.max() <= TOL, e.max()
+    want, _ = oracle.project_fp64(vol, (1, 1, 1), P, 512, 512)
+    for kernel in (L.KERNEL_CELLS, L.KERNEL_GATHER):
+        for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
+            gpu = ctx.project(v, P, 512, 512, Settings(accum=accum, kernel=kernel))
+            e = rel_err(gpu, want)
+            assert e.max() <= TOL, (kernel, accum, e.max())
     v.release()
+
+
+def test_cells_kernel_rejects_unsupported_settings(ctx):
+    m, vol, P, _ = golden_cases()[0]
+    for bad in (dict(interpolate=False), dict(volume_upsampling=2), dict(interp_mode=L.INTERP_TEXTURE)):
+        with pytest.raises(L.CtlcuError) as e:
+            ctx.project_volume(VoxelVolume(vol, m["voxel"]), P, 8, 8, Settings(kernel=L.KERNEL_CELLS, **bad))
+        assert e.value.status == L.ERR_INVALID_ARGUMENT
 
 
 def test_c2_linearity_at_full_size(ctx):
