@@ -400,7 +400,9 @@ void job_args(ProjectArgs& a, const ctlcu_settings* s, uint32_t V, uint32_t M, u
     a.tiles_per_vm = a.tiles_x * ((R + kTileY - 1) / kTileY);
     a.rays_x = s->rays_per_pixel[0];
     a.rays_y = s->rays_per_pixel[1];
-    a.vm_group = 8;
+    a.vm_group = CTLCU_VM_GROUP;
+    a.n_views = V;
+    a.view_groups = (V + kViewsPerBlock - 1) / kViewsPerBlock;
 }
 
 VolumeEntry* find_volume(ctlcu_ctx* ctx, uint64_t h)

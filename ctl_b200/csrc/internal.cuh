@@ -15,12 +15,39 @@ namespace ctlcu {
 // OpenCL CLK_ADDRESS_CLAMP border of the reference (border colour 0).
 constexpr int kPad = 2;
 
-// Detector tile handled by one thread block: 16 x 16 pixels, each warp an
-// 8 (channels) x 4 (rows) patch so that the 32 rays of a warp are neighbours
-// and their samples share cache lines.
-constexpr int kTileX = 16;
-constexpr int kTileY = 16;
-constexpr int kBlock = kTileX * kTileY;
+// Compile-time tuning of the sample loops (defaults are the measured best).
+#ifndef CTLCU_VIEWS_PER_BLOCK
+#define CTLCU_VIEWS_PER_BLOCK 2  // views sharing one thread block (1, 2 or 4)
+#endif
+#ifndef CTLCU_CELL_MINB
+#define CTLCU_CELL_MINB 5  // resident blocks per SM the register budget is sized for
+#endif
+#ifndef CTLCU_CELL_UNROLL
+#define CTLCU_CELL_UNROLL 4  // samples per partial sum
+#endif
+#ifndef CTLCU_LANES_X
+#define CTLCU_LANES_X 4  // lanes of a warp along the channels (8: 8x4 patch, 4: 4x8, 16: 16x2)
+#endif
+#ifndef CTLCU_VM_GROUP
+#define CTLCU_VM_GROUP 8  // view groups per chunk in the block order
+#endif
+
+// A thread block holds 256 rays: one detector tile of kTileX x kTileY pixels
+// for each of kViewsPerBlock consecutive views of one module.  Adjacent views
+// of a scan see a tile through nearly the same part of the volume, so their
+// rays share cached cells.  Each warp is a kLanesX x kLanesY pixel patch of
+// one view, so its 32 rays are neighbours.
+constexpr int kBlock = 256;
+constexpr int kViewsPerBlock = CTLCU_VIEWS_PER_BLOCK;
+constexpr int kTileX = kViewsPerBlock <= 2 ? 16 : 8;
+constexpr int kTileY = kBlock / (kTileX * kViewsPerBlock);
+constexpr int kWarpsPerView = kBlock / 32 / kViewsPerBlock;
+constexpr int kLanesX = CTLCU_LANES_X;
+constexpr int kLanesY = 32 / kLanesX;
+constexpr int kWarpsX = kTileX / kLanesX;
+static_assert(kViewsPerBlock == 1 || kViewsPerBlock == 2 || kViewsPerBlock == 4, "views per block");
+static_assert(kTileX % kLanesX == 0 && kTileY % kLanesY == 0, "lane patch must tile the block tile");
+static_assert(kWarpsX * (kTileY / kLanesY) == kWarpsPerView, "warps must cover the tile exactly");
 
 // Error bits raised by kernels into the context's device flag word.
 constexpr int kFlagSingular = 1;   // a projection matrix with singular / non-finite M
@@ -60,7 +87,9 @@ struct ProjectArgs {
     uint32_t csy, csz;        // cell strides (cells per row, per slice)
     uint32_t cmax;            // last valid cell index
     uint32_t ckoff;           // kMagicBits * (1 + csy + csz) mod 2^32
-    uint32_t vm_group;        // blocks cover `vm_group` consecutive view-modules per tile
+    uint32_t vm_group;        // view groups per chunk of the block order
+    uint32_t n_views;         // views (n_vm / n_modules)
+    uint32_t view_groups;     // ceil(n_views / kViewsPerBlock)
     const ViewGeom* geom;     // [n_vm]
     float* out;               // [n_vm][rows][channels]
     uint32_t channels, rows;

@@ -268,9 +268,14 @@ __device__ __forceinline__ void march_nearest(const ProjectArgs& a, const Ray& r
 // A sample that lands exactly between two cells may take either of them; both
 // give the same interpolated value.  The cell index is clamped to the array as
 // a guard; the loop bounds already keep every sample inside it.
+struct CellCache {
+    uint32_t idx = 0xffffffffu;  // cell whose coefficients c0..c7 hold
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f;
+};
+
 __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, float2 kk, float2 bxy,
                                              float bz, float2 dxy, float dz, uint32_t sy, uint32_t sz,
-                                             uint32_t koff, uint32_t cmax)
+                                             uint32_t koff, uint32_t cmax, CellCache& cc)
 {
     const float2 magic2 = make_float2(kMagic, kMagic);
     const float2 nmagic2 = make_float2(-kMagic, -kMagic);
@@ -285,20 +290,25 @@ __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, flo
     const float hz = fmaf(fz, -1.0f, vz);
     uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz - koff;
     idx = min(idx, cmax);
-    const char* p = cells + (size_t)idx * kCellBytes;
-    float c0, c1, c2, c3, c4, c5, c6, c7;
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(c0), "=f"(c1), "=f"(c2), "=f"(c3), "=f"(c4), "=f"(c5), "=f"(c6), "=f"(c7)
-        : "l"(p));
+    // consecutive samples of a ray often fall in the same cell: reload only on a change
+    if (idx != cc.idx) {
+        const char* p = cells + (size_t)idx * kCellBytes;
+        asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=f"(cc.c0), "=f"(cc.c1), "=f"(cc.c2), "=f"(cc.c3), "=f"(cc.c4), "=f"(cc.c5),
+                       "=f"(cc.c6), "=f"(cc.c7)
+                     : "l"(p));
+        cc.idx = idx;
+    }
     // (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
     const float2 hx2 = make_float2(hxy.x, hxy.x);
-    const float2 ea = __ffma2_rn(hx2, make_float2(c2, c3), make_float2(c0, c1));
-    const float2 eb = __ffma2_rn(hx2, make_float2(c6, c7), make_float2(c4, c5));
+    const float2 ea = __ffma2_rn(hx2, make_float2(cc.c2, cc.c3), make_float2(cc.c0, cc.c1));
+    const float2 eb = __ffma2_rn(hx2, make_float2(cc.c6, cc.c7), make_float2(cc.c4, cc.c5));
     const float2 g = __ffma2_rn(make_float2(hxy.y, hxy.y), eb, ea);
     return fmaf(hz, g.y, g.x);
 }
 
-// Sample loop over the coefficient cells, four samples per partial sum.
+// Sample loop over the coefficient cells, CTLCU_CELL_UNROLL samples per
+// partial sum (FP32) handed to the accumulator.
 template <Accum ACC>
 __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
@@ -310,20 +320,19 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
     const uint32_t sy = a.csy, sz = a.csz, koff = a.ckoff, cmax = a.cmax;
     const float2 one2 = make_float2(1.0f, 1.0f);
     float2 kk = make_float2(0.0f, 0.0f);
+    CellCache cc;
     int k = 0;
-    for (; k + 4 <= r.n; k += 4) {
-        float part = cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
-        kk = __fadd2_rn(kk, one2);
-        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
-        kk = __fadd2_rn(kk, one2);
-        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
-        kk = __fadd2_rn(kk, one2);
-        part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax);
-        kk = __fadd2_rn(kk, one2);
+    for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
+        float part = 0.0f;
+#pragma unroll
+        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
+            part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax, cc);
+            kk = __fadd2_rn(kk, one2);
+        }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax));
+        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax, cc));
         kk = __fadd2_rn(kk, one2);
     }
 }
@@ -342,27 +351,34 @@ __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r
 
 __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
 {
-    // Blocks run in order (group of vm_group view-modules, tile, view-module in
-    // group): blocks resident at the same time cover one detector tile of
-    // neighbouring views, whose rays cross nearly the same part of the volume.
+    // Block order: chunks of vm_group view groups; within a chunk (module,
+    // tile, view group).  Blocks resident at the same time then cover the same
+    // tiles of neighbouring views, whose rays cross nearly the same part of
+    // the volume.
     const uint32_t b = blockIdx.x;
     const uint32_t G = a.vm_group;
-    const uint32_t per_group = G * a.tiles_per_vm;
-    const uint32_t g = b / per_group;
-    const uint32_t first = g * G;
-    const uint32_t gsize = min(G, a.n_vm - first);
-    const uint32_t r = b - g * per_group;
-    const uint32_t t = r / gsize;
-    vm = first + (r - t * gsize);
-    const uint32_t ty = t / a.tiles_x, tx = t - ty * a.tiles_x;
+    const uint32_t T = a.tiles_per_vm;
+    const uint32_t per_chunk = G * a.n_modules * T;
+    const uint32_t c = b / per_chunk;
+    const uint32_t first = c * G;
+    const uint32_t gsize = min(G, a.view_groups - first);
+    const uint32_t r = b - c * per_chunk;
+    const uint32_t q = r / gsize;
+    const uint32_t vg = first + (r - q * gsize);
+    const uint32_t m = q / T;
+    const uint32_t t = q - m * T;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    x = tx * kTileX + (warp & 1u) * 8u + (lane & 7u);
-    y = ty * kTileY + (warp >> 1) * 4u + (lane >> 3);
-    return x < a.channels && y < a.rows;
+    const uint32_t slot = warp / kWarpsPerView, w = warp - slot * kWarpsPerView;
+    const uint32_t view = vg * kViewsPerBlock + slot;
+    vm = view * a.n_modules + m;
+    const uint32_t ty = t / a.tiles_x, tx = t - ty * a.tiles_x;
+    x = tx * kTileX + (w % kWarpsX) * kLanesX + (lane % kLanesX);
+    y = ty * kTileY + (w / kWarpsX) * kLanesY + (lane / kLanesX);
+    return view < a.n_views && x < a.channels && y < a.rows;
 }
 
 template <typename T, Mode M, Accum ACC, bool UP>
-__global__ void __launch_bounds__(kBlock) project_kernel(const ProjectArgs a)
+__global__ void __launch_bounds__(kBlock, M == Mode::Cells ? CTLCU_CELL_MINB : 1) project_kernel(const ProjectArgs a)
 {
     uint32_t vm, x, y;
     if (!pixel_of(a, vm, x, y))
@@ -455,7 +471,7 @@ cudaError_t launch_acc(const ProjectArgs& a, Mode mode, int dtype, dim3 grid, cu
 
 cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype, cudaStream_t s)
 {
-    const uint64_t blocks = (uint64_t)a.n_vm * a.tiles_per_vm;
+    const uint64_t blocks = (uint64_t)a.view_groups * a.n_modules * a.tiles_per_vm;
     if (blocks == 0)
         return cudaSuccess;
     if (blocks > 0x7fffffffull)
@@ -471,7 +487,7 @@ cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype
 
 cudaError_t launch_count(const ProjectArgs& a, Mode mode, cudaStream_t s)
 {
-    const uint64_t blocks = (uint64_t)a.n_vm * a.tiles_per_vm;
+    const uint64_t blocks = (uint64_t)a.view_groups * a.n_modules * a.tiles_per_vm;
     if (blocks == 0)
         return cudaSuccess;
     if (blocks > 0x7fffffffull)
