@@ -247,8 +247,8 @@ int ensure_cells(ctlcu_ctx* ctx, VolumeEntry& v)
     if (v.cells)
         return CTLCU_OK;
     const int n[3] = { (int)v.desc.n[0], (int)v.desc.n[1], (int)v.desc.n[2] };
-    const size_t ncell = (size_t)(n[0] + 2 * kPad - 1) * (n[1] + 2 * kPad - 1) * (n[2] + 2 * kPad - 1);
-    const size_t bytes = ncell * kCellBytes;
+    const CellLayout L = cell_layout(n);
+    const size_t bytes = (size_t)L.count * kCellBytes;
     if (ctx->budget && ctx->used + bytes > ctx->budget)
         return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY,
                     "cell array of %zu bytes exceeds the memory budget (%llu of %llu bytes used)", bytes,
@@ -259,7 +259,7 @@ int ensure_cells(ctlcu_ctx* ctx, VolumeEntry& v)
         CU_TRY(ctx, cudaMalloc(&v.cells, bytes));
     v.cell_bytes = bytes;
     ctx->used += bytes;
-    CU_TRY(ctx, launch_build_cells(v.data, n, v.desc.dtype, v.cells, ctx->stream));
+    CU_TRY(ctx, launch_build_cells(v.data, n, v.desc.dtype, L, v.cells, ctx->stream));
     ++ctx->launches;
     return CTLCU_OK;
 }
@@ -373,11 +373,11 @@ int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, Project
             return r;
         mode = Mode::Cells;
         a.cells = v.cells;
-        const uint32_t cx = a.ext[0] - 1, cy = a.ext[1] - 1, cz = a.ext[2] - 1;
-        a.csy = cx;
-        a.csz = cx * cy;
-        a.cmax = cx * cy * cz - 1;
-        a.ckoff = kMagicBits * (1u + a.csy + a.csz);  // mod 2^32
+        const int n[3] = { (int)d.n[0], (int)d.n[1], (int)d.n[2] };
+        const CellLayout L = cell_layout(n);
+        a.csy = L.sy;
+        a.csz = L.sz;
+        a.cmax = L.max_index;
     }
     a.sy = a.ext[0];
     a.sz = a.ext[0] * a.ext[1];

@@ -69,6 +69,38 @@ constexpr uint32_t kMagicBits = 0x4B400000u;
 // Bytes per cell of the coefficient cell array (8 floats).
 constexpr int kCellBytes = 32;
 
+// Layout of the cell array of a volume with n voxels per axis: cells span
+// padded voxels, (n + 2 kPad - 1) per axis, x fastest, row stride sy, slice
+// stride sz.  sz is padded so that 1 + sy + sz is a multiple of 1024; then
+// kMagicBits * (1 + sy + sz) = 0 mod 2^32, and the index of the cell whose
+// per-axis magic sums have bit patterns bx, by, bz is exactly
+// bx + by sy + bz sz in 32-bit arithmetic.
+struct CellLayout {
+    uint32_t cx, cy, cz;  // cells per axis
+    uint32_t sy, sz;      // strides (cells)
+    uint64_t count;       // cells allocated (sz * cz)
+    uint32_t max_index;   // index of the last real cell
+};
+
+inline CellLayout cell_layout(const int n[3])
+{
+    CellLayout L;
+    L.cx = (uint32_t)(n[0] + 2 * kPad - 1);
+    L.cy = (uint32_t)(n[1] + 2 * kPad - 1);
+    L.cz = (uint32_t)(n[2] + 2 * kPad - 1);
+    L.sy = L.cx;
+    const uint32_t base = L.cx * L.cy;
+    const uint32_t e = (1024u - ((1u + L.sy + base) & 1023u)) & 1023u;
+    L.sz = base + e;
+    L.count = (uint64_t)L.sz * L.cz;
+    L.max_index = (L.cz - 1) * L.sz + (L.cy - 1) * L.sy + (L.cx - 1);
+    return L;
+}
+
+#ifndef CTLCU_CELL_PREFETCH
+#define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
+#endif
+
 enum class Mode : int { Trilinear = 0, Nearest = 1, Texture = 2, Cells = 3 };
 enum class Accum : int { F64 = 0, Kahan = 1, F32 = 2 };
 
@@ -86,7 +118,6 @@ struct ProjectArgs {
     const void* cells;        // Mode::Cells: coefficient cells, x fastest
     uint32_t csy, csz;        // cell strides (cells per row, per slice)
     uint32_t cmax;            // last valid cell index
-    uint32_t ckoff;           // kMagicBits * (1 + csy + csz) mod 2^32
     uint32_t vm_group;        // view groups per chunk of the block order
     uint32_t n_views;         // views (n_vm / n_modules)
     uint32_t view_groups;     // ceil(n_views / kViewsPerBlock)
@@ -109,7 +140,8 @@ cudaError_t launch_count(const ProjectArgs& a, Mode mode, cudaStream_t s);
 cudaError_t launch_pad_convert(const float* src, void* dst, const int n[3], int dtype, cudaStream_t s);
 cudaError_t launch_mean(const void* padded, const int n[3], int dtype, double* sum_out, cudaStream_t s);
 cudaError_t launch_mean_volume(const double* sum, double count, float* dst_padded, cudaStream_t s);
-cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, void* cells, cudaStream_t s);
+cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, const CellLayout& L,
+                               void* cells, cudaStream_t s);
 cudaError_t launch_unpad_upsample(const void* padded, const int n[3], int dtype, int f, void* dst,
                                   cudaStream_t s);
 

@@ -273,9 +273,20 @@ struct CellCache {
     float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f;
 };
 
+// Cell index of the sample at step kk (the cell layout makes the magic
+// offsets cancel, see CellLayout), clamped to the array.
+__device__ __forceinline__ uint32_t cell_index(float2 kk, float2 bxy, float bz, float2 dxy, float dz,
+                                               uint32_t sy, uint32_t sz, uint32_t cmax)
+{
+    const float2 txy = __fadd2_rn(__ffma2_rn(kk, dxy, bxy), make_float2(kMagic, kMagic));
+    const float tz = __fadd_rn(fmaf(kk.x, dz, bz), kMagic);
+    const uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
+    return min(idx, cmax);
+}
+
 __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, float2 kk, float2 bxy,
                                              float bz, float2 dxy, float dz, uint32_t sy, uint32_t sz,
-                                             uint32_t koff, uint32_t cmax, CellCache& cc)
+                                             uint32_t cmax, CellCache& cc)
 {
     const float2 magic2 = make_float2(kMagic, kMagic);
     const float2 nmagic2 = make_float2(-kMagic, -kMagic);
@@ -288,7 +299,7 @@ __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, flo
     const float fz = __fadd_rn(tz, -kMagic);
     const float2 hxy = __ffma2_rn(fxy, none2, vxy);
     const float hz = fmaf(fz, -1.0f, vz);
-    uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz - koff;
+    uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
     idx = min(idx, cmax);
     // consecutive samples of a ray often fall in the same cell: reload only on a change
     if (idx != cc.idx) {
@@ -317,22 +328,29 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
     const float bz = (float)r.base[2];
     const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
     const float dz = (float)r.step[2];
-    const uint32_t sy = a.csy, sz = a.csz, koff = a.ckoff, cmax = a.cmax;
+    const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
     const float2 one2 = make_float2(1.0f, 1.0f);
     float2 kk = make_float2(0.0f, 0.0f);
     CellCache cc;
     int k = 0;
     for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
         float part = 0.0f;
+#if CTLCU_CELL_PREFETCH > 0
+        {
+            const float ahead = (float)CTLCU_CELL_PREFETCH;
+            const uint32_t pi = cell_index(__fadd2_rn(kk, make_float2(ahead, ahead)), bxy, bz, dxy, dz, sy, sz, cmax);
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(cells + (size_t)pi * kCellBytes));
+        }
+#endif
 #pragma unroll
         for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
-            part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax, cc);
+            part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
             kk = __fadd2_rn(kk, one2);
         }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, koff, cmax, cc));
+        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
         kk = __fadd2_rn(kk, one2);
     }
 }
@@ -378,7 +396,7 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
 }
 
 template <typename T, Mode M, Accum ACC, bool UP>
-__global__ void __launch_bounds__(kBlock, M == Mode::Cells ? CTLCU_CELL_MINB : 1) project_kernel(const ProjectArgs a)
+__global__ void __launch_bounds__(kBlock, M == Mode::Cells ? CTLCU_CELL_MINB : 3) project_kernel(const ProjectArgs a)
 {
     uint32_t vm, x, y;
     if (!pixel_of(a, vm, x, y))

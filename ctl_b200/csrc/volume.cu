@@ -114,8 +114,8 @@ __global__ void upsample_kernel(const T* __restrict__ padded, int nx, int ny, in
 //   (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
 // so the sampler evaluates f with three packed f32x2 FMAs and one FMA.
 template <typename T>
-__global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey, int ez,
-                                   float4* __restrict__ cells)
+__global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey, int ez, uint32_t csy,
+                                   uint32_t csz, float4* __restrict__ cells)
 {
     const int cx = ex - 1, cy = ey - 1, cz = ez - 1;
     const size_t total = (size_t)cx * cy * cz;
@@ -147,8 +147,9 @@ __global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey,
                     Cyz += sy_ * sz_ * t;
                     Cxyz += sx * sy_ * sz_ * t;
                 }
-        cells[2 * i] = make_float4((float)(C0 * 0.125), (float)(Cz * 0.25), (float)(Cx * 0.25), (float)(Cxz * 0.5));
-        cells[2 * i + 1] = make_float4((float)(Cy * 0.25), (float)(Cyz * 0.5), (float)(Cxy * 0.5), (float)Cxyz);
+        const size_t c = (size_t)x + (size_t)csy * y + (size_t)csz * z;
+        cells[2 * c] = make_float4((float)(C0 * 0.125), (float)(Cz * 0.25), (float)(Cx * 0.25), (float)(Cxz * 0.5));
+        cells[2 * c + 1] = make_float4((float)(Cy * 0.25), (float)(Cyz * 0.5), (float)(Cxy * 0.5), (float)Cxyz);
     }
 }
 
@@ -192,14 +193,19 @@ cudaError_t launch_mean_volume(const double* sum, double count, float* dst_padde
     return cudaGetLastError();
 }
 
-cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, void* cells, cudaStream_t s)
+cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, const CellLayout& L,
+                               void* cells, cudaStream_t s)
 {
     const int ex = n[0] + 2 * kPad, ey = n[1] + 2 * kPad, ez = n[2] + 2 * kPad;
     const unsigned g = grid_for((size_t)(ex - 1) * (ey - 1) * (ez - 1));
+    // the stride padding between slices is never sampled; keep it zero
+    cudaError_t e = cudaMemsetAsync(cells, 0, L.count * kCellBytes, s);
+    if (e != cudaSuccess)
+        return e;
     switch (dtype) {
-    case 0: build_cells_kernel<float><<<g, 256, 0, s>>>((const float*)padded, ex, ey, ez, (float4*)cells); break;
-    case 1: build_cells_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16*)padded, ex, ey, ez, (float4*)cells); break;
-    case 2: build_cells_kernel<__half><<<g, 256, 0, s>>>((const __half*)padded, ex, ey, ez, (float4*)cells); break;
+    case 0: build_cells_kernel<float><<<g, 256, 0, s>>>((const float*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
+    case 1: build_cells_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
+    case 2: build_cells_kernel<__half><<<g, 256, 0, s>>>((const __half*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
