@@ -37,15 +37,20 @@ constexpr int kPad = 2;
 // of a scan see a tile through nearly the same part of the volume, so their
 // rays share cached cells.  Each warp is a kLanesX x kLanesY pixel patch of
 // one view, so its 32 rays are neighbours.
-constexpr int kBlock = 256;
+#ifndef CTLCU_BLOCK
+#define CTLCU_BLOCK 256  // threads per block (256, 512 or 1024)
+#endif
+constexpr int kBlock = CTLCU_BLOCK;
 constexpr int kViewsPerBlock = CTLCU_VIEWS_PER_BLOCK;
-constexpr int kTileX = kViewsPerBlock <= 2 ? 16 : 8;
+constexpr int kTileX = (kViewsPerBlock <= 2 || kBlock >= 512) ? 16 : 8;
 constexpr int kTileY = kBlock / (kTileX * kViewsPerBlock);
 constexpr int kWarpsPerView = kBlock / 32 / kViewsPerBlock;
 constexpr int kLanesX = CTLCU_LANES_X;
 constexpr int kLanesY = 32 / kLanesX;
 constexpr int kWarpsX = kTileX / kLanesX;
-static_assert(kViewsPerBlock == 1 || kViewsPerBlock == 2 || kViewsPerBlock == 4, "views per block");
+static_assert(kViewsPerBlock >= 1 && kViewsPerBlock <= 8 && (kViewsPerBlock & (kViewsPerBlock - 1)) == 0,
+              "views per block");
+static_assert(kBlock == 256 || kBlock == 512 || kBlock == 1024, "block size");
 static_assert(kTileX % kLanesX == 0 && kTileY % kLanesY == 0, "lane patch must tile the block tile");
 static_assert(kWarpsX * (kTileY / kLanesY) == kWarpsPerView, "warps must cover the tile exactly");
 
@@ -75,10 +80,18 @@ constexpr int kCellBytes = 32;
 // kMagicBits * (1 + sy + sz) = 0 mod 2^32, and the index of the cell whose
 // per-axis magic sums have bit patterns bx, by, bz is exactly
 // bx + by sy + bz sz in 32-bit arithmetic.
+//
+// With CTLCU_CELL_ZFAST the roles of x and z are swapped: z is the fastest
+// axis (stride 1), y has stride sy, x stride sz.  Warps are patches of
+// detector rows and channels; for scans about the z axis the rows run along
+// z, so a warp's cells then share cache lines.
+#ifndef CTLCU_CELL_ZFAST
+#define CTLCU_CELL_ZFAST 0
+#endif
 struct CellLayout {
     uint32_t cx, cy, cz;  // cells per axis
-    uint32_t sy, sz;      // strides (cells)
-    uint64_t count;       // cells allocated (sz * cz)
+    uint32_t sy, sz;      // strides (cells) of y and of the slowest axis
+    uint64_t count;       // cells allocated
     uint32_t max_index;   // index of the last real cell
 };
 
@@ -88,14 +101,37 @@ inline CellLayout cell_layout(const int n[3])
     L.cx = (uint32_t)(n[0] + 2 * kPad - 1);
     L.cy = (uint32_t)(n[1] + 2 * kPad - 1);
     L.cz = (uint32_t)(n[2] + 2 * kPad - 1);
-    L.sy = L.cx;
-    const uint32_t base = L.cx * L.cy;
+    const uint32_t fast = CTLCU_CELL_ZFAST ? L.cz : L.cx, slow = CTLCU_CELL_ZFAST ? L.cx : L.cz;
+    L.sy = fast;
+    const uint32_t base = fast * L.cy;
     const uint32_t e = (1024u - ((1u + L.sy + base) & 1023u)) & 1023u;
     L.sz = base + e;
-    L.count = (uint64_t)L.sz * L.cz;
-    L.max_index = (L.cz - 1) * L.sz + (L.cy - 1) * L.sy + (L.cx - 1);
+    L.count = (uint64_t)L.sz * slow;
+    L.max_index = (slow - 1) * L.sz + (L.cy - 1) * L.sy + (fast - 1);
     return L;
 }
+
+// Linear cell index from per-axis indices (or their magic-sum bit patterns).
+__host__ __device__ __forceinline__ uint32_t cell_linear(uint32_t ix, uint32_t iy, uint32_t iz, uint32_t sy,
+                                                         uint32_t sz)
+{
+#if CTLCU_CELL_ZFAST
+    return iz + iy * sy + ix * sz;
+#else
+    return ix + iy * sy + iz * sz;
+#endif
+}
+
+#ifndef CTLCU_CELL_CACHE
+#define CTLCU_CELL_CACHE 2  // 0: load every sample; 1: load on cell change (branch); 2: predicated load;
+                            // 3: texture fetch on change
+#endif
+#ifndef CTLCU_CELL_RAYS
+#define CTLCU_CELL_RAYS 1  // rays per thread in the cell kernel (1 or 2)
+#endif
+#ifndef CTLCU_CELL2_MINB
+#define CTLCU_CELL2_MINB 8  // resident 128-thread blocks per SM for two rays per thread
+#endif
 
 #ifndef CTLCU_CELL_PREFETCH
 #define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
@@ -116,6 +152,7 @@ struct ProjectArgs {
     double corner[3];         // low corner of that grid (mm)
     double increment;         // step length (mm)
     const void* cells;        // Mode::Cells: coefficient cells, x fastest
+    cudaTextureObject_t cell_tex;  // the same cells as a linear float4 texture (0 if absent)
     uint32_t csy, csz;        // cell strides (cells per row, per slice)
     uint32_t cmax;            // last valid cell index
     uint32_t vm_group;        // view groups per chunk of the block order

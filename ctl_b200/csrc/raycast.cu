@@ -280,11 +280,12 @@ __device__ __forceinline__ uint32_t cell_index(float2 kk, float2 bxy, float bz, 
 {
     const float2 txy = __fadd2_rn(__ffma2_rn(kk, dxy, bxy), make_float2(kMagic, kMagic));
     const float tz = __fadd_rn(fmaf(kk.x, dz, bz), kMagic);
-    const uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
+    const uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
     return min(idx, cmax);
 }
 
-__device__ __forceinline__ float cell_sample(const char* __restrict__ cells, float2 kk, float2 bxy,
+__device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const char* __restrict__ cells, float2 kk,
+                                             float2 bxy,
                                              float bz, float2 dxy, float dz, uint32_t sy, uint32_t sz,
                                              uint32_t cmax, CellCache& cc)
 {
@@ -299,9 +300,38 @@ __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, flo
     const float fz = __fadd_rn(tz, -kMagic);
     const float2 hxy = __ffma2_rn(fxy, none2, vxy);
     const float hz = fmaf(fz, -1.0f, vz);
-    uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
+    uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
     idx = min(idx, cmax);
     // consecutive samples of a ray often fall in the same cell: reload only on a change
+#if CTLCU_CELL_CACHE == 0
+    {
+        const char* p = cells + (size_t)idx * kCellBytes;
+        asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=f"(cc.c0), "=f"(cc.c1), "=f"(cc.c2), "=f"(cc.c3), "=f"(cc.c4), "=f"(cc.c5),
+                       "=f"(cc.c6), "=f"(cc.c7)
+                     : "l"(p));
+    }
+#elif CTLCU_CELL_CACHE == 3
+    if (idx != cc.idx) {
+        // through the texture pipeline: two float4 texels per cell
+        const float4 lo = tex1Dfetch<float4>(ctex, (int)(2 * idx));
+        const float4 hi = tex1Dfetch<float4>(ctex, (int)(2 * idx + 1));
+        cc.c0 = lo.x; cc.c1 = lo.y; cc.c2 = lo.z; cc.c3 = lo.w;
+        cc.c4 = hi.x; cc.c5 = hi.y; cc.c6 = hi.z; cc.c7 = hi.w;
+        cc.idx = idx;
+    }
+#elif CTLCU_CELL_CACHE == 2
+    {
+        // predicated load: registers keep the cached cell when the index is unchanged
+        const char* p = cells + (size_t)idx * kCellBytes;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %8, %9;\n\t"
+                     "@p ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%10];\n\t}"
+                     : "+f"(cc.c0), "+f"(cc.c1), "+f"(cc.c2), "+f"(cc.c3), "+f"(cc.c4), "+f"(cc.c5),
+                       "+f"(cc.c6), "+f"(cc.c7)
+                     : "r"(idx), "r"(cc.idx), "l"(p));
+        cc.idx = idx;
+    }
+#else
     if (idx != cc.idx) {
         const char* p = cells + (size_t)idx * kCellBytes;
         asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -310,6 +340,7 @@ __device__ __forceinline__ float cell_sample(const char* __restrict__ cells, flo
                      : "l"(p));
         cc.idx = idx;
     }
+#endif
     // (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
     const float2 hx2 = make_float2(hxy.x, hxy.x);
     const float2 ea = __ffma2_rn(hx2, make_float2(cc.c2, cc.c3), make_float2(cc.c0, cc.c1));
@@ -332,27 +363,37 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
     const float2 one2 = make_float2(1.0f, 1.0f);
     float2 kk = make_float2(0.0f, 0.0f);
     CellCache cc;
+#if CTLCU_CELL_PREFETCH > 0
+    __shared__ float prefetch_sink[kBlock];
+    const uint32_t prefetch_slot = (uint32_t)__cvta_generic_to_shared(&prefetch_sink[threadIdx.x]);
+#endif
     int k = 0;
     for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
         float part = 0.0f;
 #if CTLCU_CELL_PREFETCH > 0
         {
+            // pull the cell of sample k + PREFETCH into L1 without waiting for it:
+            // an asynchronous 4-byte copy into a scratch shared word that is never read
             const float ahead = (float)CTLCU_CELL_PREFETCH;
             const uint32_t pi = cell_index(__fadd2_rn(kk, make_float2(ahead, ahead)), bxy, bz, dxy, dz, sy, sz, cmax);
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(cells + (size_t)pi * kCellBytes));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(prefetch_slot),
+                         "l"(cells + (size_t)pi * kCellBytes));
         }
 #endif
 #pragma unroll
         for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
-            part += cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
+            part += cell_sample(a.cell_tex, cells,kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
             kk = __fadd2_rn(kk, one2);
         }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(cell_sample(cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
+        acc.add(cell_sample(a.cell_tex, cells,kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
         kk = __fadd2_rn(kk, one2);
     }
+#if CTLCU_CELL_PREFETCH > 0
+    asm volatile("cp.async.wait_all;" ::: "memory");
+#endif
 }
 
 // Sample loop, hardware texture filter (border colour 0, unnormalised coords).
@@ -367,7 +408,9 @@ __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r
     }
 }
 
-__device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
+// Pixel of thread `tid` of a kBlock-thread block.
+__device__ __forceinline__ bool pixel_of_thread(const ProjectArgs& a, uint32_t tid, uint32_t& vm, uint32_t& x,
+                                                uint32_t& y)
 {
     // Block order: chunks of vm_group view groups; within a chunk (module,
     // tile, view group).  Blocks resident at the same time then cover the same
@@ -385,7 +428,7 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
     const uint32_t vg = first + (r - q * gsize);
     const uint32_t m = q / T;
     const uint32_t t = q - m * T;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
     const uint32_t slot = warp / kWarpsPerView, w = warp - slot * kWarpsPerView;
     const uint32_t view = vg * kViewsPerBlock + slot;
     vm = view * a.n_modules + m;
@@ -393,6 +436,90 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
     x = tx * kTileX + (w % kWarpsX) * kLanesX + (lane % kLanesX);
     y = ty * kTileY + (w / kWarpsX) * kLanesY + (lane / kLanesX);
     return view < a.n_views && x < a.channels && y < a.rows;
+}
+
+__device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
+{
+    return pixel_of_thread(a, threadIdx.x, vm, x, y);
+}
+
+// Two rays per thread: the cell loops of both run interleaved, so each warp
+// keeps two independent load chains in flight.  A block of kBlock/2 threads
+// covers the same pixels as a kBlock-thread block; thread t takes the pixels
+// of threads t and t + kBlock/2 of that layout (the same pixel of two
+// neighbouring views when kViewsPerBlock is 2).
+template <Accum ACC>
+__device__ __forceinline__ void march_cells2(const ProjectArgs& a, const Ray& r0, const Ray& r1,
+                                             Accumulator<ACC>& acc0, Accumulator<ACC>& acc1)
+{
+    const char* __restrict__ cells = static_cast<const char*>(a.cells);
+    const float2 b0 = make_float2((float)r0.base[0], (float)r0.base[1]);
+    const float b0z = (float)r0.base[2];
+    const float2 d0 = make_float2((float)r0.step[0], (float)r0.step[1]);
+    const float d0z = (float)r0.step[2];
+    const float2 b1 = make_float2((float)r1.base[0], (float)r1.base[1]);
+    const float b1z = (float)r1.base[2];
+    const float2 d1 = make_float2((float)r1.step[0], (float)r1.step[1]);
+    const float d1z = (float)r1.step[2];
+    const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
+    const float2 one2 = make_float2(1.0f, 1.0f);
+    float2 kk = make_float2(0.0f, 0.0f);
+    CellCache c0, c1;
+    const int nc = min(r0.n, r1.n);
+    int k = 0;
+    for (; k + CTLCU_CELL_UNROLL <= nc; k += CTLCU_CELL_UNROLL) {
+        float p0 = 0.0f, p1 = 0.0f;
+#pragma unroll
+        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
+            p0 += cell_sample(a.cell_tex, cells,kk, b0, b0z, d0, d0z, sy, sz, cmax, c0);
+            p1 += cell_sample(a.cell_tex, cells,kk, b1, b1z, d1, d1z, sy, sz, cmax, c1);
+            kk = __fadd2_rn(kk, one2);
+        }
+        acc0.add(p0);
+        acc1.add(p1);
+    }
+    float2 kk0 = kk;
+    for (int k0 = k; k0 < r0.n; ++k0) {
+        acc0.add(cell_sample(a.cell_tex, cells,kk0, b0, b0z, d0, d0z, sy, sz, cmax, c0));
+        kk0 = __fadd2_rn(kk0, one2);
+    }
+    for (int k1 = k; k1 < r1.n; ++k1) {
+        acc1.add(cell_sample(a.cell_tex, cells,kk, b1, b1z, d1, d1z, sy, sz, cmax, c1));
+        kk = __fadd2_rn(kk, one2);
+    }
+}
+
+template <Accum ACC>
+__global__ void __launch_bounds__(kBlock / 2, CTLCU_CELL2_MINB) project_cells2_kernel(const ProjectArgs a)
+{
+    uint32_t vm0, x0, y0, vm1, x1, y1;
+    const bool ok0 = pixel_of_thread(a, threadIdx.x, vm0, x0, y0);
+    const bool ok1 = pixel_of_thread(a, threadIdx.x + kBlock / 2, vm1, x1, y1);
+    if (!ok0 && !ok1)
+        return;
+    const ViewGeom& g0 = a.geom[ok0 ? vm0 : vm1];
+    const ViewGeom& g1 = a.geom[ok1 ? vm1 : vm0];
+    const bool run0 = ok0 && g0.valid, run1 = ok1 && g1.valid;
+    Accumulator<ACC> acc0, acc1;
+    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+            const double ox = -0.5 + 0.5 * ix + rx * ix, oy = -0.5 + 0.5 * iy + ry * iy;
+            Ray r0 = setup_ray<Mode::Cells>(a, g0, (double)x0 + ox, (double)y0 + oy, a.flags);
+            Ray r1 = setup_ray<Mode::Cells>(a, g1, (double)x1 + ox, (double)y1 + oy, a.flags);
+            if (!run0)
+                r0.n = 0;
+            if (!run1)
+                r1.n = 0;
+            march_cells2<ACC>(a, r0, r1, acc0, acc1);
+        }
+    const double nrays = (double)(a.rays_x * a.rays_y);
+    if (ok0)
+        a.out[((size_t)vm0 * a.rows + y0) * a.channels + x0] =
+            run0 ? (float)(a.increment * acc0.value() / nrays) : 0.0f;
+    if (ok1)
+        a.out[((size_t)vm1 * a.rows + y1) * a.channels + x1] =
+            run1 ? (float)(a.increment * acc1.value() / nrays) : 0.0f;
 }
 
 template <typename T, Mode M, Accum ACC, bool UP>
@@ -464,6 +591,10 @@ cudaError_t launch_typed(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_
 template <Mode M, Accum ACC>
 cudaError_t launch_mode(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
 {
+    if (M == Mode::Cells && CTLCU_CELL_RAYS == 2) {
+        project_cells2_kernel<ACC><<<grid, kBlock / 2, 0, s>>>(a);
+        return cudaGetLastError();
+    }
     if (M == Mode::Texture || M == Mode::Cells) {
         project_kernel<float, M, ACC, false><<<grid, kBlock, 0, s>>>(a);
         return cudaGetLastError();

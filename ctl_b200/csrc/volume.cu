@@ -147,7 +147,7 @@ __global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey,
                     Cyz += sy_ * sz_ * t;
                     Cxyz += sx * sy_ * sz_ * t;
                 }
-        const size_t c = (size_t)x + (size_t)csy * y + (size_t)csz * z;
+        const size_t c = cell_linear((uint32_t)x, (uint32_t)y, (uint32_t)z, csy, csz);
         cells[2 * c] = make_float4((float)(C0 * 0.125), (float)(Cz * 0.25), (float)(Cx * 0.25), (float)(Cxz * 0.5));
         cells[2 * c + 1] = make_float4((float)(Cy * 0.25), (float)(Cyz * 0.5), (float)(Cxy * 0.5), (float)Cxyz);
     }
