@@ -71,6 +71,10 @@ SIGNATURES = [
                                        C.c_void_p]),
     ("ctlcu_project_batch", C.c_int, [C.c_void_p, C.POINTER(Request), C.c_uint32, C.POINTER(Settings),
                                       C.c_void_p]),
+    ("ctlcu_plan_create", C.c_int, [C.c_void_p, C.POINTER(Request), C.c_uint32, C.POINTER(Settings),
+                                    C.POINTER(C.c_void_p)]),
+    ("ctlcu_plan_launch", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("ctlcu_plan_destroy", C.c_int, [C.c_void_p]),
     ("ctlcu_sync", C.c_int, [C.c_void_p]),
     ("ctlcu_count_samples", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                       C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 using namespace ctlcu;
 
@@ -38,6 +39,7 @@ struct VolumeEntry {
     void* cells = nullptr;      // coefficient cells (CTLCU_KERNEL_CELLS), built on first use
     size_t cell_bytes = 0;
     cudaTextureObject_t cell_tex = 0;  // linear float4 texture over `cells` (texture-fetch variant)
+    uint32_t plan_refs = 0;     // plans that reference this volume (release is refused meanwhile)
     std::map<int, TexEntry> tex;  // hardware-filter copies keyed by up-sampling factor
 };
 
@@ -55,6 +57,7 @@ struct ctlcu_ctx {
     int* d_flags = nullptr;
     unsigned long long* d_counter = nullptr;
     uint64_t launches = 0;
+    cudaEvent_t order = nullptr;  // orders caller streams after volume staging on `stream`
 };
 
 namespace {
@@ -426,6 +429,17 @@ VolumeEntry* find_volume(ctlcu_ctx* ctx, uint64_t h)
     return it == ctx->vols.end() ? nullptr : &it->second;
 }
 
+// Cell arrays, textures and mean voxels are built on the context's stream;
+// work on another stream `st` must start after them.
+int order_after_staging(ctlcu_ctx* ctx, cudaStream_t st)
+{
+    if (st == ctx->stream)
+        return CTLCU_OK;
+    CU_TRY(ctx, cudaEventRecord(ctx->order, ctx->stream));
+    CU_TRY(ctx, cudaStreamWaitEvent(st, ctx->order, 0));
+    return CTLCU_OK;
+}
+
 // Setup + projection on `s` with device pmats/out.  Scratch comes from the
 // stream-ordered pool, so concurrent calls on different streams do not share it.
 int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const double* d_pm,
@@ -435,6 +449,9 @@ int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, cons
     Mode mode;
     int dtype;
     int r = volume_args(ctx, v, s, a, mode, dtype);
+    if (r)
+        return r;
+    r = order_after_staging(ctx, st);
     if (r)
         return r;
     job_args(a, s, V, M, C, R);
@@ -504,6 +521,117 @@ int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const d
     return CTLCU_OK;
 }
 
+// ---- batches --------------------------------------------------------------------------------
+
+struct BatchPrep {
+    bool persistent = false;        // all requests go through the persistent cell kernel
+    std::vector<BatchSetup> setups; // per request
+    std::vector<BatchReq> reqs;     // per request (a.geom set at upload)
+    std::vector<uint32_t> first_vm; // per request
+    uint32_t total_vm = 0, total_items = 0;
+    Accum acc = Accum::F64;
+};
+
+struct BatchDevice {
+    ViewGeom* geom = nullptr;
+    BatchSetup* setups = nullptr;
+    BatchReq* reqs = nullptr;
+    unsigned int* counter = nullptr;
+};
+
+// Validate the requests and, when the settings select the cell kernel, build
+// the per-request launch arguments (building cell arrays as needed).
+int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, const ctlcu_settings* s,
+                  BatchPrep& bp)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        const ctlcu_request& q = requests[i];
+        int r = check_job(ctx, q.n_views, q.n_modules, q.channels, q.rows);
+        if (r)
+            return r;
+        if (!find_volume(ctx, q.volume))
+            return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "request %u: unknown volume handle %llu", i,
+                        (unsigned long long)q.volume);
+        if (!q.pmats || !q.out || !is_device_ptr(q.pmats) || !is_device_ptr(q.out))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u: pmats/out must be device memory", i);
+    }
+    bp.persistent = s->interpolate && s->interp_mode == CTLCU_INTERP_SOFTWARE && s->volume_upsampling == 1 &&
+                    s->kernel != CTLCU_KERNEL_GATHER;
+    if (!bp.persistent)
+        return CTLCU_OK;
+    bp.acc = (Accum)s->accum;
+    uint64_t vm = 0, items = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const ctlcu_request& q = requests[i];
+        BatchReq br = {};
+        Mode mode;
+        int dtype;
+        int r = volume_args(ctx, *find_volume(ctx, q.volume), s, br.a, mode, dtype);
+        if (r)
+            return r;
+        if (mode != Mode::Cells)
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u does not take the cell kernel", i);
+        job_args(br.a, s, q.n_views, q.n_modules, q.channels, q.rows);
+        br.a.out = q.out;
+        br.a.flags = ctx->d_flags;
+        br.a.counter = nullptr;
+        br.first_item = (uint32_t)items;
+        br.items = br.a.view_groups * br.a.n_modules * br.a.tiles_per_vm;
+        bp.first_vm.push_back((uint32_t)vm);
+        bp.setups.push_back(BatchSetup{ q.pmats, (uint32_t)vm, q.n_modules });
+        bp.reqs.push_back(br);
+        vm += (uint64_t)q.n_views * q.n_modules;
+        items += br.items;
+        if (vm > 0x7fffffffull || items > 0x7fffffffull)
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "batch too large");
+    }
+    bp.total_vm = (uint32_t)vm;
+    bp.total_items = (uint32_t)items;
+    return CTLCU_OK;
+}
+
+int upload_batch(ctlcu_ctx* ctx, BatchPrep& bp, cudaStream_t st, bool pooled, BatchDevice& bd)
+{
+    const size_t n = bp.reqs.size();
+    auto alloc = [&](void** p, size_t bytes) {
+        return pooled ? cudaMallocAsync(p, bytes, st) : cudaMalloc(p, bytes);
+    };
+    CU_TRY(ctx, alloc((void**)&bd.geom, sizeof(ViewGeom) * (size_t)bp.total_vm));
+    CU_TRY(ctx, alloc((void**)&bd.setups, sizeof(BatchSetup) * n));
+    CU_TRY(ctx, alloc((void**)&bd.reqs, sizeof(BatchReq) * n));
+    CU_TRY(ctx, alloc((void**)&bd.counter, sizeof(unsigned int)));
+    for (size_t i = 0; i < n; ++i)
+        bp.reqs[i].a.geom = bd.geom + bp.first_vm[i];
+    CU_TRY(ctx, cudaMemcpyAsync(bd.setups, bp.setups.data(), sizeof(BatchSetup) * n, cudaMemcpyHostToDevice, st));
+    CU_TRY(ctx, cudaMemcpyAsync(bd.reqs, bp.reqs.data(), sizeof(BatchReq) * n, cudaMemcpyHostToDevice, st));
+    return CTLCU_OK;
+}
+
+int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, const ctlcu_settings*,
+                  cudaStream_t st)
+{
+    const uint32_t n = (uint32_t)bp.reqs.size();
+    CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int), st));
+    CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
+    int blocks = 0;
+    CU_TRY(ctx, launch_batch_cells(bd.reqs, n, bp.total_items, bp.acc, bd.counter, &blocks, st));
+    ctx->launches += 2;
+    return CTLCU_OK;
+}
+
+void free_batch(BatchDevice& bd, cudaStream_t st, bool pooled)
+{
+    void* ptrs[4] = { bd.geom, bd.setups, bd.reqs, bd.counter };
+    for (void* p : ptrs)
+        if (p) {
+            if (pooled)
+                cudaFreeAsync(p, st);
+            else
+                cudaFree(p);
+        }
+    bd = BatchDevice{};
+}
+
 }  // namespace
 
 extern "C" {
@@ -547,6 +675,7 @@ int ctlcu_create(int device, ctlcu_ctx** out)
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->order, cudaEventDisableTiming) != cudaSuccess ||
         cudaMalloc(&ctx->d_flags, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(ctx->d_flags, 0, sizeof(int)) != cudaSuccess) {
@@ -576,6 +705,8 @@ int ctlcu_destroy(ctlcu_ctx* ctx)
         cudaStreamSynchronize(ctx->stream);
         cudaFree(ctx->d_flags);
         cudaFree(ctx->d_counter);
+        if (ctx->order)
+            cudaEventDestroy(ctx->order);
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -648,6 +779,9 @@ int ctlcu_volume_release(ctlcu_ctx* ctx, uint64_t handle)
     VolumeEntry* v = find_volume(ctx, handle);
     if (!v)
         return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)handle);
+    if (v->plan_refs)
+        return fail(ctx, CTLCU_ERR_BUSY, "volume %llu is used by %u plan(s); destroy them first",
+                    (unsigned long long)handle, v->plan_refs);
     cudaSetDevice(ctx->device);
     // work already queued on other streams may still read it
     cudaDeviceSynchronize();
@@ -737,21 +871,142 @@ int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t 
         return r;
     cudaSetDevice(ctx->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-    for (uint32_t i = 0; i < n_requests; ++i) {
-        const ctlcu_request& q = requests[i];
-        r = check_job(ctx, q.n_views, q.n_modules, q.channels, q.rows);
-        if (r)
-            return r;
-        VolumeEntry* v = find_volume(ctx, q.volume);
-        if (!v)
-            return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "request %u: unknown volume handle %llu", i,
-                        (unsigned long long)q.volume);
-        if (!q.pmats || !q.out || !is_device_ptr(q.pmats) || !is_device_ptr(q.out))
-            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u: pmats/out must be device memory", i);
-        r = project_device(ctx, *v, settings, q.pmats, q.n_views, q.n_modules, q.channels, q.rows, q.out, st);
-        if (r)
-            return r;
+    BatchPrep bp;
+    r = prepare_batch(ctx, requests, n_requests, settings, bp);
+    if (r == CTLCU_OK)
+        r = order_after_staging(ctx, st);
+    if (r)
+        return r;
+    if (!bp.persistent) {
+        // settings outside the cell kernel: one launch per request
+        for (uint32_t i = 0; i < n_requests; ++i) {
+            const ctlcu_request& q = requests[i];
+            r = project_device(ctx, *find_volume(ctx, q.volume), settings, q.pmats, q.n_views, q.n_modules,
+                               q.channels, q.rows, q.out, st);
+            if (r)
+                return r;
+        }
+        return CTLCU_OK;
     }
+    BatchDevice bd;
+    r = upload_batch(ctx, bp, st, true, bd);
+    if (r == CTLCU_OK)
+        r = enqueue_batch(ctx, bp, bd, settings, st);
+    free_batch(bd, st, true);
+    return r;
+}
+
+// ---- plans: a batch captured once as a CUDA graph and replayed -------------------------------
+
+struct ctlcu_plan {
+    ctlcu_ctx* ctx = nullptr;
+    BatchPrep bp;
+    BatchDevice bd;
+    std::vector<uint64_t> volumes;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<ctlcu_request> fallback;  // requests when the batch is not persistent
+    ctlcu_settings settings{};
+};
+
+int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                      const ctlcu_settings* settings, ctlcu_plan** out)
+{
+    if (!ctx || !out)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *out = nullptr;
+    if (!requests || n_requests == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "empty batch");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    cudaSetDevice(ctx->device);
+    ctlcu_plan* p = new (std::nothrow) ctlcu_plan;
+    if (!p)
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY, "plan allocation failed");
+    p->ctx = ctx;
+    p->settings = *settings;
+    r = prepare_batch(ctx, requests, n_requests, settings, p->bp);
+    if (r == CTLCU_OK && !p->bp.persistent)
+        r = fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                 "plans need the cell kernel (software trilinear, volumeUpSampling 1)");
+    if (r == CTLCU_OK)
+        r = upload_batch(ctx, p->bp, ctx->stream, false, p->bd);
+    cudaStream_t cs = nullptr;
+    if (r == CTLCU_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+        r = fail(ctx, CTLCU_ERR_CUDA, "stream creation failed");
+    if (r == CTLCU_OK) {
+        // descriptors must be on the device before the graph is first replayed
+        cudaStreamSynchronize(ctx->stream);
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed to start");
+        else {
+            const uint64_t before = ctx->launches;
+            r = enqueue_batch(ctx, p->bp, p->bd, settings, cs);
+            ctx->launches = before;  // counted per replay instead
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(cs, &g);
+            if (r == CTLCU_OK && e != cudaSuccess)
+                r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+            p->graph = g;
+            if (r == CTLCU_OK && cudaGraphInstantiate(&p->exec, g, 0) != cudaSuccess)
+                r = fail(ctx, CTLCU_ERR_CUDA, "graph instantiation failed");
+        }
+    }
+    if (cs)
+        cudaStreamDestroy(cs);
+    if (r) {
+        if (p->exec)
+            cudaGraphExecDestroy(p->exec);
+        if (p->graph)
+            cudaGraphDestroy(p->graph);
+        free_batch(p->bd, ctx->stream, false);
+        delete p;
+        return r;
+    }
+    for (uint32_t i = 0; i < n_requests; ++i) {
+        p->volumes.push_back(requests[i].volume);
+        ++find_volume(ctx, requests[i].volume)->plan_refs;
+    }
+    *out = p;
+    return CTLCU_OK;
+}
+
+int ctlcu_plan_launch(ctlcu_plan* plan, void* stream)
+{
+    if (!plan)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    ctlcu_ctx* ctx = plan->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    CU_TRY(ctx, cudaGraphLaunch(plan->exec, st));
+    ctx->launches += 2;
+    return CTLCU_OK;
+}
+
+int ctlcu_plan_destroy(ctlcu_plan* plan)
+{
+    if (!plan)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    ctlcu_ctx* ctx = plan->ctx;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaDeviceSynchronize();
+        if (plan->exec)
+            cudaGraphExecDestroy(plan->exec);
+        if (plan->graph)
+            cudaGraphDestroy(plan->graph);
+        free_batch(plan->bd, ctx->stream, false);
+        for (uint64_t h : plan->volumes) {
+            VolumeEntry* v = find_volume(ctx, h);
+            if (v && v->plan_refs)
+                --v->plan_refs;
+        }
+    }
+    delete plan;
     return CTLCU_OK;
 }
 

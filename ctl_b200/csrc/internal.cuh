@@ -169,7 +169,28 @@ struct ProjectArgs {
     unsigned long long* counter;  // sample count (count kernel only)
 };
 
+// One request of a batched setup (device array).
+struct BatchSetup {
+    const double* pmats;  // n_vm * 12 doubles
+    uint32_t first_vm;    // first global view-module index of this request
+    uint32_t n_modules;
+};
+
+// One request of a batched projection (device array): its launch arguments
+// (geom pointing at its ViewGeom entries) and its range of work items.
+struct BatchReq {
+    ProjectArgs a;
+    uint32_t first_item;  // first work item (block) of this request
+    uint32_t items;       // work items of this request
+};
+
 // Launchers (raycast.cu / setup.cu / volume.cu).  All asynchronous on `s`.
+cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t total, ViewGeom* geom,
+                               int* flags, cudaStream_t s);
+// Persistent cell-kernel launch over all work items of a batch; `counter`
+// must be zero at launch.  Returns the grid size used in *blocks.
+cudaError_t launch_batch_cells(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Accum acc,
+                               unsigned int* counter, int* blocks, cudaStream_t s);
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,
                          double* qr_out, double* src_out, int* flags, cudaStream_t s);
 cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype, cudaStream_t s);

@@ -408,15 +408,14 @@ __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r
     }
 }
 
-// Pixel of thread `tid` of a kBlock-thread block.
-__device__ __forceinline__ bool pixel_of_thread(const ProjectArgs& a, uint32_t tid, uint32_t& vm, uint32_t& x,
-                                                uint32_t& y)
+// Pixel of thread `tid` of work item (block) `b` of kBlock threads.
+__device__ __forceinline__ bool pixel_of_item(const ProjectArgs& a, uint32_t b, uint32_t tid, uint32_t& vm,
+                                              uint32_t& x, uint32_t& y)
 {
     // Block order: chunks of vm_group view groups; within a chunk (module,
     // tile, view group).  Blocks resident at the same time then cover the same
     // tiles of neighbouring views, whose rays cross nearly the same part of
     // the volume.
-    const uint32_t b = blockIdx.x;
     const uint32_t G = a.vm_group;
     const uint32_t T = a.tiles_per_vm;
     const uint32_t per_chunk = G * a.n_modules * T;
@@ -438,9 +437,81 @@ __device__ __forceinline__ bool pixel_of_thread(const ProjectArgs& a, uint32_t t
     return view < a.n_views && x < a.channels && y < a.rows;
 }
 
+__device__ __forceinline__ bool pixel_of_thread(const ProjectArgs& a, uint32_t tid, uint32_t& vm, uint32_t& x,
+                                                uint32_t& y)
+{
+    return pixel_of_item(a, blockIdx.x, tid, vm, x, y);
+}
+
 __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uint32_t& x, uint32_t& y)
 {
     return pixel_of_thread(a, threadIdx.x, vm, x, y);
+}
+
+// The rays of work item `b` for thread `tid`, cell kernel (FP32 cells).
+template <Accum ACC>
+__device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uint32_t tid)
+{
+    uint32_t vm, x, y;
+    if (!pixel_of_item(a, b, tid, vm, x, y))
+        return;
+    const ViewGeom& g = a.geom[vm];
+    float* dst = a.out + ((size_t)vm * a.rows + y) * a.channels + x;
+    if (!g.valid) {
+        *dst = 0.0f;
+        return;
+    }
+    Accumulator<ACC> acc;
+    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+            const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
+            const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
+            march_cells<ACC>(a, setup_ray<Mode::Cells>(a, g, px, py, a.flags), acc);
+        }
+    *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
+}
+
+// Persistent batch kernel: blocks take work items in order from `counter`
+// until all requests' items are done.  Work items of one request are its
+// blocks in the order of the single-request launch, so blocks running at the
+// same time work on neighbouring views of one volume.
+template <Accum ACC>
+__global__ void __launch_bounds__(kBlock, CTLCU_CELL_MINB)
+    batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter)
+{
+    __shared__ ProjectArgs sa;
+    __shared__ uint32_t s_item, s_local;
+    static_assert(sizeof(ProjectArgs) % 4 == 0, "word copy");
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t it = atomicAdd(counter, 1u);
+            uint32_t lo = 0;
+            if (it < total) {
+                uint32_t hi = n_reqs - 1;  // last request with first_item <= it
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) / 2;
+                    if (reqs[mid].first_item <= it)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                s_local = it - reqs[lo].first_item;
+            }
+            s_item = it < total ? lo : 0xffffffffu;
+        }
+        __syncthreads();
+        const uint32_t r = s_item;
+        if (r == 0xffffffffu)
+            return;
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&reqs[r].a);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+        for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
+            dst[i] = src[i];
+        __syncthreads();
+        cells_item<ACC>(sa, s_local, threadIdx.x);
+        __syncthreads();
+    }
 }
 
 // Two rays per thread: the cell loops of both run interleaved, so each warp
@@ -630,6 +701,41 @@ cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype
     case Accum::F64: return launch_acc<Accum::F64>(a, mode, dtype, grid, s);
     case Accum::Kahan: return launch_acc<Accum::Kahan>(a, mode, dtype, grid, s);
     case Accum::F32: return launch_acc<Accum::F32>(a, mode, dtype, grid, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+namespace {
+template <Accum ACC>
+cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter,
+                               int* blocks, cudaStream_t s)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<ACC>, kBlock, 0);
+    if (e != cudaSuccess)
+        return e;
+    uint64_t grid = (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
+    if (grid > total)
+        grid = total;
+    *blocks = (int)grid;
+    batch_cells_kernel<ACC><<<(unsigned)grid, kBlock, 0, s>>>(reqs, n_reqs, total, counter);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_batch_cells(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Accum acc,
+                               unsigned int* counter, int* blocks, cudaStream_t s)
+{
+    if (total_items == 0 || n_reqs == 0)
+        return cudaSuccess;
+    switch (acc) {
+    case Accum::F64: return launch_batch_typed<Accum::F64>(reqs, n_reqs, total_items, counter, blocks, s);
+    case Accum::Kahan: return launch_batch_typed<Accum::Kahan>(reqs, n_reqs, total_items, counter, blocks, s);
+    case Accum::F32: return launch_batch_typed<Accum::F32>(reqs, n_reqs, total_items, counter, blocks, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -24,17 +24,12 @@ __device__ double det3(double a, double b, double c, double d, double e, double 
     return a * (e * i - h * f) - b * (d * i - g * f) + c * (d * h - g * e);
 }
 
-__global__ void setup_kernel(const double* __restrict__ pmats, uint32_t n_views, uint32_t n_modules,
-                             ViewGeom* __restrict__ geom, double* __restrict__ qr_out,
-                             double* __restrict__ src_out, int* flags)
+// Geometry of one (view, module): P its matrix, P0 the view's module-0 matrix.
+// Writes *out; the packed QR to qr (if not null) and the source to src (if not null).
+__device__ void view_setup_one(const double* __restrict__ P, const double* __restrict__ P0,
+                               ViewGeom* __restrict__ out, double* __restrict__ qr, double* __restrict__ src_out,
+                               int* flags)
 {
-    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n_views * n_modules)
-        return;
-    const uint32_t view = idx / n_modules;
-    const double* P = pmats + (size_t)idx * 12;
-    const double* P0 = pmats + (size_t)view * n_modules * 12;
-
     // source position from module 0: null vector of P by cofactors
     // (projectionmatrix.cpp:264-275)
     const double hom = -det3(P0[0], P0[1], P0[2], P0[4], P0[5], P0[6], P0[8], P0[9], P0[10]);
@@ -120,28 +115,73 @@ __global__ void setup_kernel(const double* __restrict__ pmats, uint32_t n_views,
         g.src[k] = singular ? 0.0 : src[k];
     g.valid = singular ? 0 : 1;
     g.pad_ = 0;
-    geom[idx] = g;
+    *out = g;
     if (singular && flags)
         atomicOr(flags, kFlagSingular);
 
-    if (qr_out) {
-        double* q = qr_out + (size_t)idx * 15;
+    if (qr) {
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j)
-                q[3 * i + j] = Q[i][j];
-        q[9] = R[0][0];
-        q[10] = R[0][1];
-        q[11] = R[0][2];
-        q[12] = R[1][1];
-        q[13] = R[1][2];
-        q[14] = R[2][2];
+                qr[3 * i + j] = Q[i][j];
+        qr[9] = R[0][0];
+        qr[10] = R[0][1];
+        qr[11] = R[0][2];
+        qr[12] = R[1][1];
+        qr[13] = R[1][2];
+        qr[14] = R[2][2];
     }
-    if (src_out && idx == view * n_modules)
+    if (src_out)
         for (int k = 0; k < 3; ++k)
-            src_out[3 * (size_t)view + k] = src[k];
+            src_out[k] = src[k];
+}
+
+__global__ void setup_kernel(const double* __restrict__ pmats, uint32_t n_views, uint32_t n_modules,
+                             ViewGeom* __restrict__ geom, double* __restrict__ qr_out,
+                             double* __restrict__ src_out, int* flags)
+{
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n_views * n_modules)
+        return;
+    const uint32_t view = idx / n_modules;
+    view_setup_one(pmats + (size_t)idx * 12, pmats + (size_t)view * n_modules * 12, geom + idx,
+                   qr_out ? qr_out + (size_t)idx * 15 : nullptr,
+                   (src_out && idx == view * n_modules) ? src_out + 3 * (size_t)view : nullptr, flags);
+}
+
+// All view-modules of a batch: entry i of requests j covers global indices
+// first_vm[j] .. first_vm[j] + n_vm[j] - 1.
+__global__ void batch_setup_kernel(const BatchSetup* __restrict__ reqs, uint32_t n_reqs, uint32_t total,
+                                   ViewGeom* __restrict__ geom, int* flags)
+{
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total)
+        return;
+    uint32_t lo = 0, hi = n_reqs - 1;  // last request with first_vm <= idx
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) / 2;
+        if (reqs[mid].first_vm <= idx)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const BatchSetup& q = reqs[lo];
+    const uint32_t local = idx - q.first_vm;
+    const uint32_t view = local / q.n_modules;
+    view_setup_one(q.pmats + (size_t)local * 12, q.pmats + (size_t)view * q.n_modules * 12, geom + idx,
+                   nullptr, nullptr, flags);
 }
 
 }  // namespace
+
+cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t total, ViewGeom* geom,
+                               int* flags, cudaStream_t s)
+{
+    if (total == 0)
+        return cudaSuccess;
+    const uint32_t threads = 128;
+    batch_setup_kernel<<<(total + threads - 1) / threads, threads, 0, s>>>(reqs, n_reqs, total, geom, flags);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,
                          double* qr_out, double* src_out, int* flags, cudaStream_t s)

@@ -218,6 +218,29 @@ class Volume:
             self.handle = 0
 
 
+class Plan:
+    """A captured batch (ctlcu_plan): launch() replays setup + persistent projection."""
+
+    def __init__(self, ctx: "Context", handle, requests):
+        self.ctx = ctx
+        self.h = handle
+        self.requests = list(requests)  # keeps the device tensors alive
+
+    def launch(self, stream: int = 0) -> None:
+        self.ctx._check(self.ctx.lib.ctlcu_plan_launch(self.h, C.c_void_p(stream or None)))
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx._check(self.ctx.lib.ctlcu_plan_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One CUDA device: stream, memory budget, resident volumes, projection calls."""
 
@@ -314,10 +337,8 @@ class Context:
                                                   C.c_void_p(_ptr(out))))
         return out
 
-    def project_batch(self, requests: Sequence[tuple], settings: Optional[Settings] = None,
-                      stream: int = 0) -> None:
-        """requests: (Volume, device pmats tensor (V,M,3,4) f64, device out tensor (V,M,R,C) f32)."""
-        settings = settings or Settings()
+    @staticmethod
+    def _requests(requests: Sequence[tuple]):
         arr = (L.Request * len(requests))()
         for i, (vol, P, out) in enumerate(requests):
             arr[i].volume = vol.handle
@@ -325,9 +346,26 @@ class Context:
             arr[i].out = _ptr(out)
             arr[i].n_views, arr[i].n_modules = int(P.shape[0]), int(P.shape[1])
             arr[i].rows, arr[i].channels = int(out.shape[2]), int(out.shape[3])
+        return arr
+
+    def project_batch(self, requests: Sequence[tuple], settings: Optional[Settings] = None,
+                      stream: int = 0) -> None:
+        """requests: (Volume, device pmats tensor (V,M,3,4) f64, device out tensor (V,M,R,C) f32).
+        All requests' views run in one persistent launch."""
+        settings = settings or Settings()
+        arr = self._requests(requests)
         st = settings.to_c()
         self._check(self.lib.ctlcu_project_batch(self.h, arr, len(requests), C.byref(st),
                                                  C.c_void_p(stream or None)))
+
+    def plan(self, requests: Sequence[tuple], settings: Optional[Settings] = None) -> "Plan":
+        """A batch captured once as a CUDA graph; Plan.launch() replays it."""
+        settings = settings or Settings()
+        arr = self._requests(requests)
+        st = settings.to_c()
+        h = C.c_void_p()
+        self._check(self.lib.ctlcu_plan_create(self.h, arr, len(requests), C.byref(st), C.byref(h)))
+        return Plan(self, h, requests)
 
     def sync(self) -> None:
         self._check(self.lib.ctlcu_sync(self.h))

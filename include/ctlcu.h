@@ -167,6 +167,20 @@ CTLCU_API int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc
 CTLCU_API int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
                         const ctlcu_settings* settings, void* stream);
 
+/*
+ * Plans: a batch prepared once (descriptors on the device, cell arrays built)
+ * and captured as a CUDA graph of its setup and persistent projection
+ * launches; each ctlcu_plan_launch replays it on `stream`.  The requests'
+ * pmats/out pointers are fixed in the plan -- update their contents in place
+ * between launches.  Plans need the cell kernel; their volumes cannot be
+ * released (CTLCU_ERR_BUSY) until the plan is destroyed.
+ */
+typedef struct ctlcu_plan ctlcu_plan;
+CTLCU_API int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                                const ctlcu_settings* settings, ctlcu_plan** plan);
+CTLCU_API int ctlcu_plan_launch(ctlcu_plan* plan, void* stream);
+CTLCU_API int ctlcu_plan_destroy(ctlcu_plan* plan);
+
 /* Wait for the context's stream; reports a deferred device-side error
  * (CTLCU_ERR_SINGULAR_GEOMETRY) raised by an earlier asynchronous call. */
 CTLCU_API int ctlcu_sync(ctlcu_ctx* ctx);

@@ -225,3 +225,81 @@ def test_uniform_cube_chord_full_detector(ctx):
     out = ctx.project_volume(VoxelVolume(vol, (1, 1, 1)), P, 257, 257)
     assert abs(out[0, 0, 128, 128] - mu * n) <= 2 * mu * 0.3
     assert out[0, 0, 0, 0] == 0.0
+
+
+# ---- batches and plans ------------------------------------------------------------------------
+
+def _uneven_requests(ctx, rng_seed=5):
+    """Small batch of uneven volumes / views / detectors (the batched configuration in miniature)."""
+    import torch
+    rng = np.random.default_rng(rng_seed)
+    reqs, meta = [], []
+    for i in range(5):
+        shape = tuple(int(s) for s in rng.choice([24, 32, 40], 3))
+        vox = float(rng.choice([2.0, 3.0]))
+        vol = Ph.ellipsoid_phantom(shape, (vox, vox, vox), 4, seed=100 + i)
+        V = int(rng.integers(2, 7))
+        C, R = int(rng.choice([24, 40])), int(rng.choice([16, 32]))
+        P = G.circular_flat(V, 750.0, 1000.0, G.FlatDetector(C, R, 2.0, 2.0), start=float(rng.uniform(0, 6)))
+        v = ctx.volume(VoxelVolume(vol, (vox,) * 3))
+        dP = torch.from_numpy(np.ascontiguousarray(P)).cuda()
+        out = torch.zeros((V, 1, R, C), device="cuda")
+        reqs.append((v, dP, out))
+        meta.append((vol, vox, P, C, R))
+    return reqs, meta
+
+
+def test_persistent_batch_matches_oracle_and_single_calls(ctx):
+    reqs, meta = _uneven_requests(ctx)
+    ctx.project_batch(reqs, Settings())
+    ctx.sync()
+    for (v, dP, out), (vol, vox, P, C, R) in zip(reqs, meta):
+        single = ctx.project(v, P, C, R, Settings())
+        got = out.cpu().numpy()
+        np.testing.assert_allclose(got, single, rtol=1e-6, atol=1e-7)
+        want, _ = oracle.project_fp64(vol, (vox,) * 3, P, C, R)
+        assert rel_err(got, want).max() <= TOL
+    for v, _, _ in reqs:
+        v.release()
+
+
+def test_plan_replay_and_in_place_update(ctx):
+    import torch
+    reqs, meta = _uneven_requests(ctx, rng_seed=9)
+    plan = ctx.plan(reqs, Settings())
+    plan.launch()
+    ctx.sync()
+    first = [out.clone() for _, _, out in reqs]
+    for _, _, out in reqs:
+        out.zero_()
+    plan.launch()
+    ctx.sync()
+    for (_, _, out), f in zip(reqs, first):
+        assert torch.equal(out, f)
+    # new geometry written in place is picked up by the next replay
+    v0, dP0, out0 = reqs[0]
+    vol, vox, P, C, R = meta[0]
+    P2 = G.circular_flat(P.shape[0], 750.0, 1000.0, G.FlatDetector(C, R, 2.0, 2.0), start=1.234)
+    dP0.copy_(torch.from_numpy(P2))
+    plan.launch()
+    ctx.sync()
+    want, _ = oracle.project_fp64(vol, (vox,) * 3, P2, C, R)
+    assert rel_err(out0.cpu().numpy(), want).max() <= TOL
+    # a volume in a plan cannot be released until the plan is gone
+    with pytest.raises(L.CtlcuError) as e:
+        v0.release()
+    assert e.value.status == L.ERR_BUSY
+    plan.close()
+    for v, _, _ in reqs:
+        v.release()
+
+
+def test_batch_outside_cell_kernel_falls_back_per_request(ctx):
+    reqs, meta = _uneven_requests(ctx, rng_seed=3)
+    s = Settings(interpolate=False)
+    ctx.project_batch(reqs, s)
+    ctx.sync()
+    for (v, dP, out), (vol, vox, P, C, R) in zip(reqs, meta):
+        want, _ = oracle.project_fp64(vol, (vox,) * 3, P, C, R, interpolate=False)
+        assert rel_err(out.cpu().numpy(), want).max() <= TOL
+        v.release()
