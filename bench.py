@@ -318,6 +318,150 @@ def run_ours(args):
     return 0
 
 
+# ---- the other configurations (extra lines; the headline is the 256^3 -> 512^2 one above) ------
+
+def _time_device(fn, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in ev:
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def _line(metric, value, unit, ms, args, config, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+         "vs_baseline": None, "data": "synthetic (seeded ellipsoid phantoms, seeded geometry)", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_single_config(args, name):
+    """c1 / c3: one volume, all views per step, resident; several sample-loop forms."""
+    import torch
+
+    from ctl_b200 import _lib as L
+    from ctl_b200 import workloads as W
+    from ctl_b200.projector import Context, Settings, VoxelVolume
+    job = W.c1() if name == "c1" else W.c3()
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    V, M = job.pmats.shape[:2]
+    dP = torch.from_numpy(job.pmats).cuda()
+    out = torch.empty((V, M, job.rows, job.channels), device="cuda")
+    forms = {"cells_fp64": Settings(), "cells_kahan": Settings(accum=L.ACCUM_KAHAN),
+             "cells_fp32": Settings(accum=L.ACCUM_FP32), "gather_fp64": Settings(kernel=L.KERNEL_GATHER),
+             "texture_fp64": Settings(interp_mode=L.INTERP_TEXTURE)}
+    storages = {"f32": L.F32, "bf16": L.BF16}
+    results = {}
+    for sname, storage in storages.items():
+        vol = ctx.volume(VoxelVolume(job.volume, job.voxel), storage)
+        for fname, s in forms.items():
+            if storage == L.BF16 and fname == "texture_fp64":
+                continue
+            ms = _time_device(lambda: ctx.project(vol, dP, job.channels, job.rows, s, out=out, stream=ctx.stream),
+                              args.steps, args.warmup, stream)
+            results[f"{sname}_{fname}"] = V / (statistics.mean(ms) / 1e3)
+        if sname == "f32":
+            samples = ctx.count_samples(vol, job.pmats, job.channels, job.rows)
+        vol.release()
+    best = results["f32_cells_fp64"]
+    ms = V / best * 1e3
+    extra = {"forms_views_per_s": results, "samples_per_step": samples,
+             "gsamples_per_s": samples / (ms / 1e3) / 1e9}
+    if name == "c1" and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            vol_h = job.volume if isinstance(job.volume, np.ndarray) else job.volume.cpu().numpy()
+            t0 = time.perf_counter()
+            oracle.project_ref(vol_h, job.voxel, job.pmats, job.channels, job.rows, threads=os.cpu_count())
+            dt = time.perf_counter() - t0
+            extra["cpu_baseline"] = {"value": V / dt, "unit": "projections/s", "cores": os.cpu_count(),
+                                     "kind": "reference", "sample": f"all {V} views, {dt:.1f} s"}
+    _line(f"projections/s, {job.name}", best, "projections/s", ms, args,
+          {"workload": job.name, "views_per_step": V, "modules": M}, **extra)
+    ctx.close()
+
+
+def run_c4(args):
+    """64 uneven volumes: one persistent launch replayed from a CUDA graph vs 64 sequential calls."""
+    import torch
+
+    from ctl_b200 import _lib as L
+    from ctl_b200 import workloads as W
+    from ctl_b200.projector import Context, Settings, VoxelVolume
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    jobs = W.c4()
+    total_views = sum(j.pmats.shape[0] for j in jobs)
+    for storage_name, storage in (("f32", L.F32), ("bf16", L.BF16)):
+        vols = [ctx.volume(VoxelVolume(j.volume, j.voxel), storage) for j in jobs]
+        reqs = []
+        for j, v in zip(jobs, vols):
+            V, M = j.pmats.shape[:2]
+            reqs.append((v, torch.from_numpy(j.pmats).cuda(), torch.empty((V, M, j.rows, j.channels), device="cuda")))
+        plan = ctx.plan(reqs, Settings())
+        ms_plan = _time_device(lambda: plan.launch(ctx.stream), args.steps, args.warmup, stream)
+
+        def sequential(kernel):
+            s = Settings(kernel=kernel)
+            for (v, P, out), j in zip(reqs, jobs):
+                ctx.project(v, P, j.channels, j.rows, s, out=out, stream=ctx.stream)
+        ms_seq = _time_device(lambda: sequential(L.KERNEL_CELLS), max(2, args.steps // 3), 1, stream)
+        ms_plain = _time_device(lambda: sequential(L.KERNEL_GATHER), max(2, args.steps // 3), 1, stream)
+        plan.close()
+        v_plan = total_views / (statistics.mean(ms_plan) / 1e3)
+        _line(f"projections/s, 64 uneven volumes batched ({storage_name} storage)", v_plan, "projections/s",
+              statistics.mean(ms_plan), args,
+              {"workload": "64 volumes (edges 96-256), 30-360 views each, detectors 256^2-768x512",
+               "views_per_step": total_views, "storage": storage_name},
+              sequential_cells_views_per_s=total_views / (statistics.mean(ms_seq) / 1e3),
+              sequential_plain_gather_views_per_s=total_views / (statistics.mean(ms_plain) / 1e3))
+        for v in vols:
+            v.release()
+        del reqs
+        torch.cuda.empty_cache()
+    ctx.close()
+
+
+def run_c5(args):
+    """DRR serving: capacity, then latency percentiles at 2000 requests/s offered."""
+    import torch
+
+    from ctl_b200 import _lib as L
+    from ctl_b200 import workloads as W
+    from ctl_b200.projector import Context, Settings, VoxelVolume
+    from ctl_b200.serving import DRRServer, poisson_requests
+    ctx = Context(0)
+    vols = [ctx.volume(VoxelVolume(v, (1.0, 1.0, 1.0)), L.BF16) for v in W.c5_volumes()]
+    kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS}[args.kernel]
+    server = DRRServer(ctx, vols, 256, 256, Settings(kernel=kernel), streams=3, max_batch=256,
+                       budget_bytes=40 * 10**9)
+    server.warm_up()
+    base = W.c5_base_view()
+    # capacity: all requests offered at once
+    cap = server.run(poisson_requests(1e7, 2000, len(vols), base, seed=50)).summary()
+    rate = 2000.0
+    n = int(rate * args.serve_seconds)
+    at = server.run(poisson_requests(rate, n, len(vols), base, seed=51)).summary()
+    under = min(0.8 * cap["throughput_req_s"], rate)
+    below = server.run(poisson_requests(under, int(under * args.serve_seconds), len(vols), base, seed=52)).summary()
+    _line("p99 DRR latency at 2000 requests/s (8 x 256^3 BF16, 1-16 views of 256^2)", at["p99_ms"], "ms",
+          at["p50_ms"], args,
+          {"workload": "8 resident 256^3 BF16 volumes; Poisson 2000/s; 1-16 perturbed views of 256^2 @1.2 mm",
+           "budget_bytes": 40 * 10**9}, higher_is_better=False, serving_at_2000=at, capacity=cap,
+          serving_at_80pct_capacity=dict(below, offered_req_s=under))
+    for v in vols:
+        v.release()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,9 +478,18 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5"], default="c2",
+                    help="c2 (default) is the headline; the others print extra lines")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config in ("c1", "c3"):
+        return run_single_config(args, args.config)
+    if args.config == "c4":
+        return run_c4(args)
+    if args.config == "c5":
+        return run_c5(args)
     return run_ours(args)
 
 

@@ -308,6 +308,19 @@ class Context:
             return torch.empty((V, M, R, Cn), dtype=torch.float32, device=pmats.device)
         return np.empty((V, M, R, Cn), dtype=np.float32)
 
+    @staticmethod
+    def _stream_for(stream: int, *arrays) -> int:
+        """Asynchronous calls on device tensors run on torch's current stream
+        unless a stream is given, so torch's caching allocator orders the reuse
+        of their memory after our kernels."""
+        if stream:
+            return stream
+        for t in arrays:
+            if _is_cuda(t):
+                import torch
+                return torch.cuda.current_stream(t.device).cuda_stream
+        return 0
+
     def project(self, volume: Volume, pmats, channels: int, rows: int,
                 settings: Optional[Settings] = None, out=None, stream: int = 0):
         settings = settings or Settings()
@@ -316,6 +329,7 @@ class Context:
         if out is None:
             out = self._out_like(P, V, M, rows, channels)
         st = settings.to_c()
+        stream = self._stream_for(stream, P, out)
         self._check(self.lib.ctlcu_project(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(P)), V, M,
                                            int(channels), int(rows), C.c_void_p(_ptr(out)),
                                            C.c_void_p(stream or None)))
@@ -355,6 +369,7 @@ class Context:
         settings = settings or Settings()
         arr = self._requests(requests)
         st = settings.to_c()
+        stream = self._stream_for(stream, *[r[2] for r in requests])
         self._check(self.lib.ctlcu_project_batch(self.h, arr, len(requests), C.byref(st),
                                                  C.c_void_p(stream or None)))
 

@@ -1,0 +1,196 @@
+"""Continuous-batching DRR server over resident volumes.
+
+Requests (volume, a few views of arbitrary pose, one detector size) arrive
+over time, as in 2D/3D registration and simulation tools that call
+RayCasterProjector::project once per pose (examples/regist2d3d/main.cpp,
+examples/simTool/mainwindow.cpp:192-217).  Here the volumes stay resident on
+the device and requests are batched as they arrive:
+
+* admission: a request is accepted while the device memory of all accepted,
+  unfinished requests (their projection matrices and images) stays within the
+  budget; otherwise it waits in the arrival queue (or is refused if `refuse`);
+* batching: whenever one of `streams` CUDA streams is free, every queued
+  request (up to `max_batch`) goes into one persistent launch on it
+  (ctlcu_project_batch), so requests that arrive while others run are picked
+  up as soon as a stream frees and their work overlaps on the device;
+* timing: latency is arrival (host clock) to the end of the request's batch
+  on the device (CUDA event), with the device clock tied to the host clock
+  at start.
+
+The projections of a request depend only on its own inputs: the persistent
+kernel computes every work item independently, so a result is the same alone
+and in any mix (tests/test_gpu_serving.py checks this).
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .projector import Context, Settings, Volume
+
+
+@dataclass
+class DRRRequest:
+    rid: int
+    volume: int             # index into the server's volumes
+    pmats: np.ndarray       # (views, modules, 3, 4) float64
+    arrival: float          # seconds after the start of the run
+    out: object = None      # device tensor (views, modules, rows, channels), set on admission
+    done: float = -1.0      # seconds after start when the result was ready on the device
+    refused: bool = False
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+@dataclass
+class ServeStats:
+    n: int
+    completed: int
+    refused: int
+    wall_s: float
+    views: int
+    latencies_ms: List[float] = field(default_factory=list)
+    batches: int = 0
+    mean_batch: float = 0.0
+
+    def summary(self) -> dict:
+        lat = np.asarray(self.latencies_ms) if self.latencies_ms else np.zeros(1)
+        return {
+            "requests": self.n, "completed": self.completed, "refused": self.refused,
+            "throughput_req_s": self.completed / self.wall_s if self.wall_s > 0 else 0.0,
+            "throughput_views_s": self.views / self.wall_s if self.wall_s > 0 else 0.0,
+            "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+            "batches": self.batches, "mean_requests_per_batch": self.mean_batch,
+        }
+
+
+class DRRServer:
+    def __init__(self, ctx: Context, volumes: Sequence[Volume], channels: int, rows: int,
+                 settings: Optional[Settings] = None, streams: int = 2, max_batch: int = 256,
+                 budget_bytes: int = 40 * 10**9, refuse: bool = False):
+        import torch
+        self.torch = torch
+        self.ctx = ctx
+        self.volumes = list(volumes)
+        self.channels, self.rows = channels, rows
+        self.settings = settings or Settings()
+        self.streams = [torch.cuda.Stream() for _ in range(streams)]
+        self.max_batch = max_batch
+        self.refuse = refuse
+        self.budget_bytes = budget_bytes
+        if self._free_budget() <= 0:
+            raise ValueError("the resident volumes alone exceed the memory budget")
+
+    def _free_budget(self) -> int:
+        """Budget left for requests after the resident volumes (with their cell arrays)."""
+        return self.budget_bytes - sum(v.nbytes for v in self.volumes)
+
+    def _bytes(self, req: DRRRequest) -> int:
+        V, M = req.pmats.shape[:2]
+        return int(V * M * (self.rows * self.channels * 4 + 96))
+
+    def warm_up(self) -> None:
+        """Build every volume's cell array and the kernels' first launch outside timing."""
+        torch = self.torch
+        P = np.zeros((1, 1, 3, 4))
+        P[0, 0, :, :3] = np.eye(3)
+        P[0, 0, 2, 3] = 1000.0
+        # the device buffers must outlive the asynchronous launches: keep them
+        # until the stream is synchronised, and run on torch's current stream
+        # so its caching allocator orders any reuse after our kernels
+        keep = []
+        stream = torch.cuda.current_stream().cuda_stream
+        for v in self.volumes:
+            out = torch.empty((1, 1, self.rows, self.channels), device="cuda")
+            dP = torch.from_numpy(P).cuda()
+            keep.append((dP, out))
+            self.ctx.project_batch([(v, dP, out)], self.settings, stream=stream)
+        torch.cuda.synchronize()
+        self.ctx.sync()
+
+    def run(self, requests: Sequence[DRRRequest]) -> ServeStats:
+        torch = self.torch
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        pending = list(reqs)
+        pending.reverse()  # pop() takes the earliest
+        queue: List[DRRRequest] = []
+        inflight = [None] * len(self.streams)  # (batch, end_event)
+        self.budget = self._free_budget()
+        used = 0
+        done = refused = batches = batched = 0
+        torch.cuda.synchronize()
+        base = torch.cuda.Event(enable_timing=True)
+        base.record(self.streams[0])
+        base.synchronize()
+        t0 = time.perf_counter()
+        while done + refused < len(reqs):
+            now = time.perf_counter() - t0
+            # arrivals: admit into the queue while the budget allows
+            while pending and pending[-1].arrival <= now:
+                r = pending[-1]
+                need = self._bytes(r)
+                if used + need > self.budget:
+                    if self.refuse:
+                        pending.pop()
+                        r.refused = True
+                        refused += 1
+                        continue
+                    break  # wait for memory to free
+                pending.pop()
+                used += need
+                queue.append(r)
+            # completions, then new batches on free streams
+            for i, s in enumerate(self.streams):
+                slot = inflight[i]
+                if slot is not None and slot[1].query():
+                    ms = base.elapsed_time(slot[1])
+                    for r in slot[0]:
+                        r.done = ms / 1e3
+                        used -= self._bytes(r)
+                    done += len(slot[0])
+                    inflight[i] = None
+                if inflight[i] is None and queue:
+                    batch, queue = queue[: self.max_batch], queue[self.max_batch:]
+                    with torch.cuda.stream(s):
+                        # one host-to-device copy for the whole batch's matrices
+                        allP = torch.from_numpy(np.concatenate([r.pmats.reshape(-1, 12) for r in batch]))
+                        allP = allP.to("cuda", non_blocking=False)
+                        items, at = [], 0
+                        for r in batch:
+                            V, M = r.pmats.shape[:2]
+                            dP = allP[at: at + V * M].view(V, M, 3, 4)
+                            at += V * M
+                            r.out = torch.empty((V, M, self.rows, self.channels), device="cuda")
+                            items.append((self.volumes[r.volume], dP, r.out))
+                        self.ctx.project_batch(items, self.settings, stream=s.cuda_stream)
+                        ev = torch.cuda.Event(enable_timing=True)
+                        ev.record(s)
+                    inflight[i] = (batch, ev)
+                    batches += 1
+                    batched += len(batch)
+        wall = time.perf_counter() - t0
+        lat = [1e3 * r.latency for r in reqs if not r.refused]
+        views = sum(int(r.pmats.shape[0]) for r in reqs if not r.refused)
+        return ServeStats(n=len(reqs), completed=done, refused=refused, wall_s=wall, views=views,
+                          latencies_ms=lat, batches=batches, mean_batch=batched / max(batches, 1))
+
+
+def poisson_requests(rate_hz: float, n: int, n_volumes: int, base_pmats: np.ndarray, seed: int,
+                     views=(1, 16), trans_mm: float = 10.0, rot_deg: float = 5.0) -> List[DRRRequest]:
+    """Seeded Poisson arrivals; each request asks for 1-16 rigidly perturbed
+    copies of the base C-arm view (+-trans_mm, +-rot_deg)."""
+    from . import geometry as G
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n))
+    out = []
+    for i in range(n):
+        nv = int(rng.integers(views[0], views[1] + 1))
+        P = G.perturbed_views(base_pmats, nv, rng, trans_mm, rot_deg)
+        out.append(DRRRequest(rid=i, volume=int(rng.integers(0, n_volumes)), pmats=P, arrival=float(t[i])))
+    return out

@@ -1,0 +1,66 @@
+"""The continuous-batching DRR server: every request's result is the same
+alone and in the mix, and matches the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from ctl_b200 import geometry as G
+from ctl_b200 import phantom as Ph
+from ctl_b200.projector import Context, Settings, VoxelVolume
+from ctl_b200.serving import DRRServer, poisson_requests
+from tests._common import dequant_bf16, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _base_view(C=48, R=40):
+    det = G.FlatDetector(C, R, 2.4, 2.4)
+    return G.circular_flat(1, 750.0, 1200.0, det)[0]  # (modules, 3, 4)
+
+
+def test_server_results_equal_alone_and_oracle():
+    from ctl_b200 import _lib as L
+    ctx = Context(0)
+    vols = [Ph.ellipsoid_phantom((40, 40, 32), (3, 3, 3), 5, seed=20 + i) for i in range(3)]
+    handles = [ctx.volume(VoxelVolume(v, (3, 3, 3)), L.BF16) for v in vols]
+    server = DRRServer(ctx, handles, 48, 40, Settings(), streams=2, max_batch=16)
+    server.warm_up()
+    reqs = poisson_requests(4000.0, 60, len(vols), _base_view(), seed=7, views=(1, 6))
+    stats = server.run(reqs)
+    assert stats.completed == 60 and stats.refused == 0 and stats.batches >= 2
+    assert all(r.done >= r.arrival for r in reqs)
+    import torch
+    for r in reqs:
+        # the same request alone through the same batched path: identical bits
+        out = torch.zeros_like(r.out)
+        ctx.project_batch([(handles[r.volume], torch.from_numpy(r.pmats).cuda(), out)], Settings())
+        ctx.sync()
+        np.testing.assert_array_equal(r.out.cpu().numpy(), out.cpu().numpy())
+        # and through the single-request kernel
+        alone = ctx.project(handles[r.volume], r.pmats, 48, 40, Settings())
+        np.testing.assert_allclose(r.out.cpu().numpy(), alone, rtol=1e-6, atol=1e-7)
+    for r in reqs[::12]:
+        want, _ = oracle.project_fp64(dequant_bf16(vols[r.volume]), (3, 3, 3), r.pmats, 48, 40)
+        assert rel_err(r.out.cpu().numpy(), want).max() <= 1e-4
+    for h in handles:
+        h.release()
+    ctx.close()
+
+
+def test_server_admission_by_budget():
+    from ctl_b200 import _lib as L
+    ctx = Context(0)
+    vol = Ph.ellipsoid_phantom((24, 24, 24), (4, 4, 4), 3, seed=1)
+    h = ctx.volume(VoxelVolume(vol, (4, 4, 4)))
+    # budget for the volume plus about two requests' images: the rest must wait or be refused
+    per_req = 4 * (48 * 40 * 4 + 96)
+    server = DRRServer(ctx, [h], 48, 40, Settings(), streams=1, max_batch=8,
+                       budget_bytes=h.nbytes + 2 * per_req, refuse=True)
+    server.warm_up()
+    reqs = poisson_requests(1e6, 20, 1, _base_view(), seed=3, views=(4, 4))
+    stats = server.run(reqs)
+    assert stats.refused > 0 and stats.completed + stats.refused == 20
+    with pytest.raises(ValueError):
+        DRRServer(ctx, [h], 48, 40, budget_bytes=1)
+    h.release()
+    ctx.close()
