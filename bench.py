@@ -211,7 +211,8 @@ def run_ours(args):
     settings = Settings(accum={"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[args.accum],
                         storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage],
                         interp_mode=L.INTERP_TEXTURE if args.interp == "texture" else L.INTERP_SOFTWARE,
-                        kernel={"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS}[args.kernel])
+                        kernel={"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
+                                 "pairs": L.KERNEL_PAIRS}[args.kernel])
     ctx = Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     vobj = VoxelVolume(vol, VOXEL)
@@ -440,7 +441,8 @@ def run_c5(args):
     from ctl_b200.serving import DRRServer, poisson_requests
     ctx = Context(0)
     vols = [ctx.volume(VoxelVolume(v, (1.0, 1.0, 1.0)), L.BF16) for v in W.c5_volumes()]
-    kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS}[args.kernel]
+    kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
+                                 "pairs": L.KERNEL_PAIRS}[args.kernel]
     server = DRRServer(ctx, vols, 256, 256, Settings(kernel=kernel), streams=3, max_batch=256,
                        budget_bytes=40 * 10**9)
     server.warm_up()
@@ -471,7 +473,7 @@ def main():
     ap.add_argument("--accum", choices=["fp64", "kahan", "fp32"], default="fp64")
     ap.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32")
     ap.add_argument("--interp", choices=["software", "texture"], default="software")
-    ap.add_argument("--kernel", choices=["auto", "gather", "cells"], default="auto")
+    ap.add_argument("--kernel", choices=["auto", "gather", "cells", "pairs"], default="auto")
     ap.add_argument("--views", type=int, default=N_VIEWS,
                     help="views per step (360 = the configuration; fewer = a small profiling case)")
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -24,7 +24,7 @@ ERR_BUSY = 8
 F32, BF16, F16 = 0, 1, 2
 INTERP_SOFTWARE, INTERP_TEXTURE = 0, 1
 ACCUM_FP64, ACCUM_KAHAN, ACCUM_FP32 = 0, 1, 2
-KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS = 0, 1, 2
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS, KERNEL_PAIRS = 0, 1, 2, 3
 
 STATUS_NAMES = {
     OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",

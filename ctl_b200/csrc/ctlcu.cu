@@ -40,6 +40,8 @@ struct VolumeEntry {
     size_t cell_bytes = 0;
     cudaTextureObject_t cell_tex = 0;  // linear float4 texture over `cells` (texture-fetch variant)
     uint32_t plan_refs = 0;     // plans that reference this volume (release is refused meanwhile)
+    void* pairs = nullptr;      // x-pair array (CTLCU_KERNEL_PAIRS), built on first use
+    size_t pair_bytes = 0;
     std::map<int, TexEntry> tex;  // hardware-filter copies keyed by up-sampling factor
 };
 
@@ -116,9 +118,9 @@ int check_settings(ctlcu_ctx* ctx, const ctlcu_settings* s)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown interp_mode %d", s->interp_mode);
     if (s->accum < CTLCU_ACCUM_FP64 || s->accum > CTLCU_ACCUM_FP32)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown accum %d", s->accum);
-    if (s->kernel < CTLCU_KERNEL_AUTO || s->kernel > CTLCU_KERNEL_CELLS)
+    if (s->kernel < CTLCU_KERNEL_AUTO || s->kernel > CTLCU_KERNEL_PAIRS)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown kernel %d", s->kernel);
-    if (s->kernel == CTLCU_KERNEL_CELLS &&
+    if ((s->kernel == CTLCU_KERNEL_CELLS || s->kernel == CTLCU_KERNEL_PAIRS) &&
         (!s->interpolate || s->interp_mode != CTLCU_INTERP_SOFTWARE || s->volume_upsampling != 1))
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
                     "the cell kernel needs software trilinear interpolation and volumeUpSampling 1");
@@ -218,6 +220,15 @@ void free_volume(ctlcu_ctx* ctx, VolumeEntry& v)
     }
     v.cells = nullptr;
     v.cell_bytes = 0;
+    if (v.pairs) {
+        if (v.pooled)
+            cudaFreeAsync(v.pairs, ctx->stream);
+        else
+            cudaFree(v.pairs);
+        ctx->used -= std::min<uint64_t>(ctx->used, v.pair_bytes);
+    }
+    v.pairs = nullptr;
+    v.pair_bytes = 0;
     if (v.data) {
         if (v.pooled)
             cudaFreeAsync(v.data, ctx->stream);
@@ -278,6 +289,29 @@ int ensure_cells(ctlcu_ctx* ctx, VolumeEntry& v)
         td.readMode = cudaReadModeElementType;
         CU_TRY(ctx, cudaCreateTextureObject(&v.cell_tex, &rd, &td, nullptr));
     }
+    return CTLCU_OK;
+}
+
+// x-pair array of the padded volume, built once per volume on first use.
+int ensure_pairs(ctlcu_ctx* ctx, VolumeEntry& v)
+{
+    if (v.pairs)
+        return CTLCU_OK;
+    const int n[3] = { (int)v.desc.n[0], (int)v.desc.n[1], (int)v.desc.n[2] };
+    const PairLayout L = pair_layout(n);
+    const size_t bytes = (size_t)L.count * sizeof(float2);
+    if (ctx->budget && ctx->used + bytes > ctx->budget)
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY,
+                    "pair array of %zu bytes exceeds the memory budget (%llu of %llu bytes used)", bytes,
+                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    if (v.pooled)
+        CU_TRY(ctx, cudaMallocAsync(&v.pairs, bytes, ctx->stream));
+    else
+        CU_TRY(ctx, cudaMalloc(&v.pairs, bytes));
+    v.pair_bytes = bytes;
+    ctx->used += bytes;
+    CU_TRY(ctx, launch_build_pairs(v.data, n, v.desc.dtype, L, v.pairs, ctx->stream));
+    ++ctx->launches;
     return CTLCU_OK;
 }
 
@@ -384,7 +418,18 @@ int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, Project
         if (r)
             return r;
     }
-    if (mode == Mode::Trilinear && f == 1 && s->kernel != CTLCU_KERNEL_GATHER) {
+    if (mode == Mode::Trilinear && f == 1 && s->kernel == CTLCU_KERNEL_PAIRS) {
+        int r = ensure_pairs(ctx, v);
+        if (r)
+            return r;
+        mode = Mode::Pairs;
+        a.cells = v.pairs;
+        const int n[3] = { (int)d.n[0], (int)d.n[1], (int)d.n[2] };
+        const PairLayout L = pair_layout(n);
+        a.csy = L.sy;
+        a.csz = L.sz;
+        a.cmax = L.max_base;
+    } else if (mode == Mode::Trilinear && f == 1 && s->kernel != CTLCU_KERNEL_GATHER) {
         int r = ensure_cells(ctx, v);
         if (r)
             return r;
@@ -530,6 +575,7 @@ struct BatchPrep {
     std::vector<uint32_t> first_vm; // per request
     uint32_t total_vm = 0, total_items = 0;
     Accum acc = Accum::F64;
+    Mode mode = Mode::Cells;        // Cells or Pairs, the same for every request
 };
 
 struct BatchDevice {
@@ -569,8 +615,9 @@ int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, con
         int r = volume_args(ctx, *find_volume(ctx, q.volume), s, br.a, mode, dtype);
         if (r)
             return r;
-        if (mode != Mode::Cells)
+        if (mode != Mode::Cells && mode != Mode::Pairs)
             return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u does not take the cell kernel", i);
+        bp.mode = mode;
         job_args(br.a, s, q.n_views, q.n_modules, q.channels, q.rows);
         br.a.out = q.out;
         br.a.flags = ctx->d_flags;
@@ -614,7 +661,7 @@ int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, co
     CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int), st));
     CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
     int blocks = 0;
-    CU_TRY(ctx, launch_batch_cells(bd.reqs, n, bp.total_items, bp.acc, bd.counter, &blocks, st));
+    CU_TRY(ctx, launch_batch(bd.reqs, n, bp.total_items, bp.mode, bp.acc, bd.counter, &blocks, st));
     ctx->launches += 2;
     return CTLCU_OK;
 }
@@ -798,7 +845,7 @@ int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes)
     VolumeEntry* v = find_volume(ctx, handle);
     if (!v)
         return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)handle);
-    uint64_t b = v->bytes + v->cell_bytes;
+    uint64_t b = v->bytes + v->cell_bytes + v->pair_bytes;
     for (auto& t : v->tex)
         b += t.second.bytes;
     *bytes = b;

@@ -137,7 +137,35 @@ __host__ __device__ __forceinline__ uint32_t cell_linear(uint32_t ix, uint32_t i
 #define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
 #endif
 
-enum class Mode : int { Trilinear = 0, Nearest = 1, Texture = 2, Cells = 3 };
+// x-pair array: for every padded voxel (x < ext_x - 1, y, z) the float2
+// (mid, diff) = ((v[x] + v[x+1]) / 2, v[x+1] - v[x]), computed in FP64.  A
+// trilinear cell reads four entries (its two rows in y times two slices in
+// z); the x interpolation of an entry at offset h from the cell centre is
+// mid + h * diff.  8 bytes per voxel; strides padded like the cell array so
+// the magic offsets cancel.
+struct PairLayout {
+    uint32_t px, ey, ez;  // entries per row, rows, slices
+    uint32_t sy, sz;      // strides (entries)
+    uint64_t count;       // entries allocated (sz * ez)
+    uint32_t max_base;    // largest first-entry index whose 4 entries are in the array
+};
+
+inline PairLayout pair_layout(const int n[3])
+{
+    PairLayout L;
+    L.px = (uint32_t)(n[0] + 2 * kPad - 1);
+    L.ey = (uint32_t)(n[1] + 2 * kPad);
+    L.ez = (uint32_t)(n[2] + 2 * kPad);
+    L.sy = L.px;
+    const uint32_t base = L.px * L.ey;
+    const uint32_t e = (1024u - ((1u + L.sy + base) & 1023u)) & 1023u;
+    L.sz = base + e;
+    L.count = (uint64_t)L.sz * L.ez;
+    L.max_base = (uint32_t)(L.count - 1 - L.sy - L.sz);
+    return L;
+}
+
+enum class Mode : int { Trilinear = 0, Nearest = 1, Texture = 2, Cells = 3, Pairs = 4 };
 enum class Accum : int { F64 = 0, Kahan = 1, F32 = 2 };
 
 // Everything a projection launch needs, passed by value.
@@ -187,10 +215,10 @@ struct BatchReq {
 // Launchers (raycast.cu / setup.cu / volume.cu).  All asynchronous on `s`.
 cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t total, ViewGeom* geom,
                                int* flags, cudaStream_t s);
-// Persistent cell-kernel launch over all work items of a batch; `counter`
-// must be zero at launch.  Returns the grid size used in *blocks.
-cudaError_t launch_batch_cells(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Accum acc,
-                               unsigned int* counter, int* blocks, cudaStream_t s);
+// Persistent launch (Mode::Cells or Mode::Pairs) over all work items of a
+// batch; `counter` must be zero at launch.  Returns the grid size in *blocks.
+cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
+                         unsigned int* counter, int* blocks, cudaStream_t s);
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,
                          double* qr_out, double* src_out, int* flags, cudaStream_t s);
 cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype, cudaStream_t s);
@@ -200,6 +228,8 @@ cudaError_t launch_mean(const void* padded, const int n[3], int dtype, double* s
 cudaError_t launch_mean_volume(const double* sum, double count, float* dst_padded, cudaStream_t s);
 cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, const CellLayout& L,
                                void* cells, cudaStream_t s);
+cudaError_t launch_build_pairs(const void* padded, const int n[3], int dtype, const PairLayout& L,
+                               void* pairs, cudaStream_t s);
 cudaError_t launch_unpad_upsample(const void* padded, const int n[3], int dtype, int f, void* dst,
                                   cudaStream_t s);
 

@@ -143,7 +143,7 @@ __device__ __forceinline__ Ray setup_ray(const ProjectArgs& a, const ViewGeom& g
         r.step[0] = r.step[1] = r.step[2] = 0.0;
         return r;
     }
-    if (M == Mode::Cells) {
+    if (M == Mode::Cells || M == Mode::Pairs) {
         // Only samples inside the box contribute (the reference's first and last
         // samples, floor(tmin) and floor(tmax)+1, lie outside it and read zeros),
         // so the loop runs over ceil(t0) .. floor(t1).  Coordinates are
@@ -396,6 +396,84 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
 #endif
 }
 
+// x-pair entries of the current cell: rows (y, z), (y+1, z), (y, z+1), (y+1, z+1).
+struct PairCache {
+    uint32_t idx = 0xffffffffu;
+    float m00 = 0.f, d00 = 0.f, m10 = 0.f, d10 = 0.f, m01 = 0.f, d01 = 0.f, m11 = 0.f, d11 = 0.f;
+};
+
+// One sample from the x-pair array: the same cell index and centre offsets as
+// cell_sample, four 8-byte entries loaded only when the cell changes, x by
+// mid + hx diff, then y and z linearly.
+__device__ __forceinline__ float pair_sample(const char* __restrict__ pairs, float2 kk, float2 bxy, float bz,
+                                             float2 dxy, float dz, uint32_t sy, uint32_t sz, uint32_t pmax,
+                                             PairCache& pc)
+{
+    const float2 magic2 = make_float2(kMagic, kMagic);
+    const float2 nmagic2 = make_float2(-kMagic, -kMagic);
+    const float2 none2 = make_float2(-1.0f, -1.0f);
+    const float2 vxy = __ffma2_rn(kk, dxy, bxy);
+    const float vz = fmaf(kk.x, dz, bz);
+    const float2 txy = __fadd2_rn(vxy, magic2);
+    const float tz = __fadd_rn(vz, kMagic);
+    const float2 fxy = __fadd2_rn(txy, nmagic2);
+    const float fz = __fadd_rn(tz, -kMagic);
+    const float2 hxy = __ffma2_rn(fxy, none2, vxy);
+    const float hz = fmaf(fz, -1.0f, vz);
+    uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
+    idx = min(idx, pmax);
+    {
+        const char* p0 = pairs + (size_t)idx * 8;
+        const char* p1 = p0 + (size_t)sy * 8;
+        const char* p2 = p0 + (size_t)sz * 8;
+        const char* p3 = p2 + (size_t)sy * 8;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %8, %9;\n\t"
+                     "@p ld.global.nc.v2.f32 {%0, %1}, [%10];\n\t"
+                     "@p ld.global.nc.v2.f32 {%2, %3}, [%11];\n\t"
+                     "@p ld.global.nc.v2.f32 {%4, %5}, [%12];\n\t"
+                     "@p ld.global.nc.v2.f32 {%6, %7}, [%13];\n\t}"
+                     : "+f"(pc.m00), "+f"(pc.d00), "+f"(pc.m10), "+f"(pc.d10), "+f"(pc.m01), "+f"(pc.d01),
+                       "+f"(pc.m11), "+f"(pc.d11)
+                     : "r"(idx), "r"(pc.idx), "l"(p0), "l"(p1), "l"(p2), "l"(p3));
+        pc.idx = idx;
+    }
+    const float hx = hxy.x;
+    const float2 lo = make_float2(fmaf(hx, pc.d00, pc.m00), fmaf(hx, pc.d01, pc.m01));  // (y, z), (y, z+1)
+    const float2 hi = make_float2(fmaf(hx, pc.d10, pc.m10), fmaf(hx, pc.d11, pc.m11));  // (y+1, z), (y+1, z+1)
+    const float wy = hxy.y + 0.5f, wz = hz + 0.5f;
+    const float2 e = __ffma2_rn(make_float2(wy, wy), __ffma2_rn(lo, none2, hi), lo);     // z, z+1
+    return fmaf(wz, e.y - e.x, e.x);
+}
+
+// Sample loop over the x-pair array (same structure as march_cells).
+template <Accum ACC>
+__device__ __forceinline__ void march_pairs(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
+{
+    const char* __restrict__ pairs = static_cast<const char*>(a.cells);
+    const float2 bxy = make_float2((float)r.base[0], (float)r.base[1]);
+    const float bz = (float)r.base[2];
+    const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
+    const float dz = (float)r.step[2];
+    const uint32_t sy = a.csy, sz = a.csz, pmax = a.cmax;
+    const float2 one2 = make_float2(1.0f, 1.0f);
+    float2 kk = make_float2(0.0f, 0.0f);
+    PairCache pc;
+    int k = 0;
+    for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
+        float part = 0.0f;
+#pragma unroll
+        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
+            part += pair_sample(pairs, kk, bxy, bz, dxy, dz, sy, sz, pmax, pc);
+            kk = __fadd2_rn(kk, one2);
+        }
+        acc.add(part);
+    }
+    for (; k < r.n; ++k) {
+        acc.add(pair_sample(pairs, kk, bxy, bz, dxy, dz, sy, sz, pmax, pc));
+        kk = __fadd2_rn(kk, one2);
+    }
+}
+
 // Sample loop, hardware texture filter (border colour 0, unnormalised coords).
 template <Accum ACC>
 __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
@@ -449,7 +527,7 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
 }
 
 // The rays of work item `b` for thread `tid`, cell kernel (FP32 cells).
-template <Accum ACC>
+template <Mode M, Accum ACC>
 __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uint32_t tid)
 {
     uint32_t vm, x, y;
@@ -467,7 +545,11 @@ __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uin
         for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
             const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
             const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
-            march_cells<ACC>(a, setup_ray<Mode::Cells>(a, g, px, py, a.flags), acc);
+            const Ray r = setup_ray<M>(a, g, px, py, a.flags);
+            if (M == Mode::Pairs)
+                march_pairs<ACC>(a, r, acc);
+            else
+                march_cells<ACC>(a, r, acc);
         }
     *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
 }
@@ -476,7 +558,7 @@ __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uin
 // until all requests' items are done.  Work items of one request are its
 // blocks in the order of the single-request launch, so blocks running at the
 // same time work on neighbouring views of one volume.
-template <Accum ACC>
+template <Mode M, Accum ACC>
 __global__ void __launch_bounds__(kBlock, CTLCU_CELL_MINB)
     batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter)
 {
@@ -509,7 +591,7 @@ __global__ void __launch_bounds__(kBlock, CTLCU_CELL_MINB)
         for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
             dst[i] = src[i];
         __syncthreads();
-        cells_item<ACC>(sa, s_local, threadIdx.x);
+        cells_item<M, ACC>(sa, s_local, threadIdx.x);
         __syncthreads();
     }
 }
@@ -594,7 +676,8 @@ __global__ void __launch_bounds__(kBlock / 2, CTLCU_CELL2_MINB) project_cells2_k
 }
 
 template <typename T, Mode M, Accum ACC, bool UP>
-__global__ void __launch_bounds__(kBlock, M == Mode::Cells ? CTLCU_CELL_MINB : 3) project_kernel(const ProjectArgs a)
+__global__ void __launch_bounds__(kBlock, (M == Mode::Cells || M == Mode::Pairs) ? CTLCU_CELL_MINB : 3)
+    project_kernel(const ProjectArgs a)
 {
     uint32_t vm, x, y;
     if (!pixel_of(a, vm, x, y))
@@ -614,6 +697,8 @@ __global__ void __launch_bounds__(kBlock, M == Mode::Cells ? CTLCU_CELL_MINB : 3
             const Ray r = setup_ray<M>(a, g, px, py, a.flags);
             if (M == Mode::Cells)
                 march_cells<ACC>(a, r, acc);
+            else if (M == Mode::Pairs)
+                march_pairs<ACC>(a, r, acc);
             else if (M == Mode::Trilinear)
                 march_trilinear<T, ACC, UP>(a, r, acc);
             else if (M == Mode::Nearest)
@@ -666,7 +751,7 @@ cudaError_t launch_mode(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t
         project_cells2_kernel<ACC><<<grid, kBlock / 2, 0, s>>>(a);
         return cudaGetLastError();
     }
-    if (M == Mode::Texture || M == Mode::Cells) {
+    if (M == Mode::Texture || M == Mode::Cells || M == Mode::Pairs) {
         project_kernel<float, M, ACC, false><<<grid, kBlock, 0, s>>>(a);
         return cudaGetLastError();
     }
@@ -683,6 +768,7 @@ cudaError_t launch_acc(const ProjectArgs& a, Mode mode, int dtype, dim3 grid, cu
     case Mode::Nearest: return launch_mode<Mode::Nearest, ACC>(a, dtype, grid, s);
     case Mode::Texture: return launch_mode<Mode::Texture, ACC>(a, dtype, grid, s);
     case Mode::Cells: return launch_mode<Mode::Cells, ACC>(a, dtype, grid, s);
+    case Mode::Pairs: return launch_mode<Mode::Pairs, ACC>(a, dtype, grid, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -706,7 +792,7 @@ cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype
 }
 
 namespace {
-template <Accum ACC>
+template <Mode M, Accum ACC>
 cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter,
                                int* blocks, cudaStream_t s)
 {
@@ -715,28 +801,39 @@ cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t t
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<ACC>, kBlock, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<M, ACC>, kBlock, 0);
     if (e != cudaSuccess)
         return e;
     uint64_t grid = (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
     if (grid > total)
         grid = total;
     *blocks = (int)grid;
-    batch_cells_kernel<ACC><<<(unsigned)grid, kBlock, 0, s>>>(reqs, n_reqs, total, counter);
+    batch_cells_kernel<M, ACC><<<(unsigned)grid, kBlock, 0, s>>>(reqs, n_reqs, total, counter);
     return cudaGetLastError();
+}
+
+template <Mode M>
+cudaError_t launch_batch_mode(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, Accum acc,
+                              unsigned int* counter, int* blocks, cudaStream_t s)
+{
+    switch (acc) {
+    case Accum::F64: return launch_batch_typed<M, Accum::F64>(reqs, n_reqs, total, counter, blocks, s);
+    case Accum::Kahan: return launch_batch_typed<M, Accum::Kahan>(reqs, n_reqs, total, counter, blocks, s);
+    case Accum::F32: return launch_batch_typed<M, Accum::F32>(reqs, n_reqs, total, counter, blocks, s);
+    }
+    return cudaErrorInvalidValue;
 }
 }  // namespace
 
-cudaError_t launch_batch_cells(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Accum acc,
-                               unsigned int* counter, int* blocks, cudaStream_t s)
+cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
+                         unsigned int* counter, int* blocks, cudaStream_t s)
 {
     if (total_items == 0 || n_reqs == 0)
         return cudaSuccess;
-    switch (acc) {
-    case Accum::F64: return launch_batch_typed<Accum::F64>(reqs, n_reqs, total_items, counter, blocks, s);
-    case Accum::Kahan: return launch_batch_typed<Accum::Kahan>(reqs, n_reqs, total_items, counter, blocks, s);
-    case Accum::F32: return launch_batch_typed<Accum::F32>(reqs, n_reqs, total_items, counter, blocks, s);
-    }
+    if (mode == Mode::Pairs)
+        return launch_batch_mode<Mode::Pairs>(reqs, n_reqs, total_items, acc, counter, blocks, s);
+    if (mode == Mode::Cells)
+        return launch_batch_mode<Mode::Cells>(reqs, n_reqs, total_items, acc, counter, blocks, s);
     return cudaErrorInvalidValue;
 }
 

@@ -153,6 +153,25 @@ __global__ void build_cells_kernel(const T* __restrict__ padded, int ex, int ey,
     }
 }
 
+// x-pair entries (mid, diff) of the padded volume, see PairLayout.
+template <typename T>
+__global__ void build_pairs_kernel(const T* __restrict__ padded, int ex, int ey, int ez, uint32_t psy,
+                                   uint32_t psz, float2* __restrict__ pairs)
+{
+    const int px = ex - 1;
+    const size_t total = (size_t)px * ey * ez;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % px);
+        const size_t r = i / px;
+        const int y = (int)(r % ey);
+        const int z = (int)(r / ey);
+        const size_t o = (size_t)x + (size_t)ex * ((size_t)y + (size_t)ey * z);
+        const double a = (double)to_float<T>(padded[o]), b = (double)to_float<T>(padded[o + 1]);
+        pairs[(size_t)x + (size_t)psy * y + (size_t)psz * z] = make_float2((float)(0.5 * (a + b)), (float)(b - a));
+    }
+}
+
 unsigned grid_for(size_t n)
 {
     size_t b = (n + 255) / 256;
@@ -206,6 +225,23 @@ cudaError_t launch_build_cells(const void* padded, const int n[3], int dtype, co
     case 0: build_cells_kernel<float><<<g, 256, 0, s>>>((const float*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
     case 1: build_cells_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
     case 2: build_cells_kernel<__half><<<g, 256, 0, s>>>((const __half*)padded, ex, ey, ez, L.sy, L.sz, (float4*)cells); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_pairs(const void* padded, const int n[3], int dtype, const PairLayout& L,
+                               void* pairs, cudaStream_t s)
+{
+    const int ex = n[0] + 2 * kPad, ey = n[1] + 2 * kPad, ez = n[2] + 2 * kPad;
+    const unsigned g = grid_for((size_t)(ex - 1) * ey * ez);
+    cudaError_t e = cudaMemsetAsync(pairs, 0, L.count * sizeof(float2), s);
+    if (e != cudaSuccess)
+        return e;
+    switch (dtype) {
+    case 0: build_pairs_kernel<float><<<g, 256, 0, s>>>((const float*)padded, ex, ey, ez, L.sy, L.sz, (float2*)pairs); break;
+    case 1: build_pairs_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16*)padded, ex, ey, ez, L.sy, L.sz, (float2*)pairs); break;
+    case 2: build_pairs_kernel<__half><<<g, 256, 0, s>>>((const __half*)padded, ex, ey, ez, L.sy, L.sz, (float2*)pairs); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -72,7 +72,13 @@ typedef enum {
  *           polynomial about the cell centre (FP32, built on the device once
  *           per resident volume; 8x the voxel count x 4 bytes)
  */
-typedef enum { CTLCU_KERNEL_AUTO = 0, CTLCU_KERNEL_GATHER = 1, CTLCU_KERNEL_CELLS = 2 } ctlcu_kernel;
+typedef enum {
+    CTLCU_KERNEL_AUTO = 0,
+    CTLCU_KERNEL_GATHER = 1,
+    CTLCU_KERNEL_CELLS = 2,
+    CTLCU_KERNEL_PAIRS = 3  /* four 8-byte loads per cell from an x-pair array (mid, diff)
+                               per voxel: 2x the voxel count x 4 bytes */
+} ctlcu_kernel;
 
 typedef struct ctlcu_ctx ctlcu_ctx;
 

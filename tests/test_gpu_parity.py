@@ -43,10 +43,12 @@ def _oracle(m, vol, P):
     return out, S
 
 
-@pytest.mark.parametrize("kernel", [L.KERNEL_AUTO, L.KERNEL_GATHER], ids=["auto", "gather"])
+@pytest.mark.parametrize("kernel", [L.KERNEL_AUTO, L.KERNEL_GATHER, L.KERNEL_PAIRS], ids=["auto", "gather", "pairs"])
 @pytest.mark.parametrize("case", golden_cases(), ids=lambda c: c[0]["name"])
 def test_golden_cases_match_oracle_and_reference(ctx, case, kernel):
     m, vol, P, ref = case
+    if kernel == L.KERNEL_PAIRS and (not m["interpolate"] or m["upsampling"] != 1):
+        pytest.skip("the pair kernel serves software trilinear interpolation without up-sampling")
     gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"],
                              _settings(m, kernel=kernel))
     want, _ = _oracle(m, vol, P)
@@ -62,7 +64,7 @@ def test_golden_cases_match_oracle_and_reference(ctx, case, kernel):
         assert np.quantile(er, 0.999) < 1e-3 and er.mean() < 1e-4
 
 
-@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER], ids=["cells", "gather"])
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER, L.KERNEL_PAIRS], ids=["cells", "gather", "pairs"])
 @pytest.mark.parametrize("accum,tol", [(L.ACCUM_FP64, TOL), (L.ACCUM_KAHAN, TOL), (L.ACCUM_FP32, 2e-3)])
 def test_accumulation_modes(ctx, accum, tol, kernel):
     m, vol, P, _ = golden_cases()[0]
@@ -72,7 +74,7 @@ def test_accumulation_modes(ctx, accum, tol, kernel):
     assert rel_err(gpu, want).max() <= tol
 
 
-@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER], ids=["cells", "gather"])
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_GATHER, L.KERNEL_PAIRS], ids=["cells", "gather", "pairs"])
 @pytest.mark.parametrize("storage,deq", [(L.BF16, dequant_bf16), (L.F16, dequant_f16)])
 def test_reduced_precision_storage_vs_dequantised_oracle(ctx, storage, deq, kernel):
     m, vol, P, _ = golden_cases()[0]
@@ -188,7 +190,7 @@ def test_c2_full_size_views_match_oracle(ctx):
     P = _c2_geometry()[[0, 181]]
     v = ctx.volume(VoxelVolume(vol, (1, 1, 1)))
     want, _ = oracle.project_fp64(vol, (1, 1, 1), P, 512, 512)
-    for kernel in (L.KERNEL_CELLS, L.KERNEL_GATHER):
+    for kernel in (L.KERNEL_CELLS, L.KERNEL_GATHER, L.KERNEL_PAIRS):
         for accum in (L.ACCUM_FP64, L.ACCUM_KAHAN):
             gpu = ctx.project(v, P, 512, 512, Settings(accum=accum, kernel=kernel))
             e = rel_err(gpu, want)
@@ -249,12 +251,13 @@ def _uneven_requests(ctx, rng_seed=5):
     return reqs, meta
 
 
-def test_persistent_batch_matches_oracle_and_single_calls(ctx):
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_PAIRS], ids=["cells", "pairs"])
+def test_persistent_batch_matches_oracle_and_single_calls(ctx, kernel):
     reqs, meta = _uneven_requests(ctx)
-    ctx.project_batch(reqs, Settings())
+    ctx.project_batch(reqs, Settings(kernel=kernel))
     ctx.sync()
     for (v, dP, out), (vol, vox, P, C, R) in zip(reqs, meta):
-        single = ctx.project(v, P, C, R, Settings())
+        single = ctx.project(v, P, C, R, Settings(kernel=kernel))
         got = out.cpu().numpy()
         np.testing.assert_allclose(got, single, rtol=1e-6, atol=1e-7)
         want, _ = oracle.project_fp64(vol, (vox,) * 3, P, C, R)
