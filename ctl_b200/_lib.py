@@ -78,6 +78,9 @@ SIGNATURES = [
     ("ctlcu_sync", C.c_int, [C.c_void_p]),
     ("ctlcu_count_samples", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                       C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
+    ("ctlcu_autotune", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
+                                 C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_float)]),
     ("ctlcu_view_setup", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                    C.c_void_p]),
     ("ctlcu_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),

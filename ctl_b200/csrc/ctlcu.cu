@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -42,6 +43,7 @@ struct VolumeEntry {
     uint32_t plan_refs = 0;     // plans that reference this volume (release is refused meanwhile)
     void* pairs = nullptr;      // x-pair array (CTLCU_KERNEL_PAIRS), built on first use
     size_t pair_bytes = 0;
+    uint64_t handle = 0;        // 0 for the temporary volume of ctlcu_project_volume
     std::map<int, TexEntry> tex;  // hardware-filter copies keyed by up-sampling factor
 };
 
@@ -60,6 +62,8 @@ struct ctlcu_ctx {
     unsigned long long* d_counter = nullptr;
     uint64_t launches = 0;
     cudaEvent_t order = nullptr;  // orders caller streams after volume staging on `stream`
+    // autotuned sample-loop choice per (volume, channels, rows, modules)
+    std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, int> tuned;
 };
 
 namespace {
@@ -487,9 +491,27 @@ int order_after_staging(ctlcu_ctx* ctx, cudaStream_t st)
 
 // Setup + projection on `s` with device pmats/out.  Scratch comes from the
 // stream-ordered pool, so concurrent calls on different streams do not share it.
-int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const double* d_pm,
+// CTLCU_KERNEL_AUTO resolved: the autotuned choice for this volume and
+// detector if there is one, else the cell kernel where it applies.
+ctlcu_settings resolve_kernel(ctlcu_ctx* ctx, const VolumeEntry& v, const ctlcu_settings* s, uint32_t C, uint32_t R,
+                              uint32_t M)
+{
+    ctlcu_settings e = *s;
+    if (e.kernel != CTLCU_KERNEL_AUTO)
+        return e;
+    const bool fast = e.interpolate && e.interp_mode == CTLCU_INTERP_SOFTWARE && e.volume_upsampling == 1;
+    if (!fast)
+        return e;
+    auto it = ctx->tuned.find(std::make_tuple(v.handle, C, R, M));
+    e.kernel = it != ctx->tuned.end() ? it->second : CTLCU_KERNEL_CELLS;
+    return e;
+}
+
+int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s_in, const double* d_pm,
                    uint32_t V, uint32_t M, uint32_t C, uint32_t R, float* d_out, cudaStream_t st)
 {
+    const ctlcu_settings eff = resolve_kernel(ctx, v, s_in, C, R, M);
+    const ctlcu_settings* s = &eff;
     ProjectArgs a = {};
     Mode mode;
     int dtype;
@@ -606,13 +628,16 @@ int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, con
     if (!bp.persistent)
         return CTLCU_OK;
     bp.acc = (Accum)s->accum;
+    // one sample loop for the whole launch: the first request's (autotuned) choice
+    const ctlcu_settings eff = resolve_kernel(ctx, *find_volume(ctx, requests[0].volume), s, requests[0].channels,
+                                              requests[0].rows, requests[0].n_modules);
     uint64_t vm = 0, items = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const ctlcu_request& q = requests[i];
         BatchReq br = {};
         Mode mode;
         int dtype;
-        int r = volume_args(ctx, *find_volume(ctx, q.volume), s, br.a, mode, dtype);
+        int r = volume_args(ctx, *find_volume(ctx, q.volume), &eff, br.a, mode, dtype);
         if (r)
             return r;
         if (mode != Mode::Cells && mode != Mode::Pairs)
@@ -813,6 +838,7 @@ int ctlcu_volume_create(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const flo
         return fail(ctx, CTLCU_ERR_CUDA, "volume upload failed: %s", cudaGetErrorString(e));
     }
     const uint64_t h = ctx->next_handle++;
+    v.handle = h;
     ctx->vols.emplace(h, v);
     *handle = h;
     return CTLCU_OK;
@@ -834,6 +860,8 @@ int ctlcu_volume_release(ctlcu_ctx* ctx, uint64_t handle)
     cudaDeviceSynchronize();
     free_volume(ctx, *v);
     ctx->vols.erase(handle);
+    for (auto it = ctx->tuned.begin(); it != ctx->tuned.end();)
+        it = std::get<0>(it->first) == handle ? ctx->tuned.erase(it) : std::next(it);
     return CTLCU_OK;
 }
 
@@ -1117,6 +1145,110 @@ int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* s
         CU_TRY(ctx, cudaFreeAsync(d_pm, st));
     CU_TRY(ctx, cudaStreamSynchronize(st));
     *samples = n;
+    return read_flags(ctx);
+}
+
+int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings, const double* pmats,
+                   uint32_t n_views, uint32_t n_modules, uint32_t channels, uint32_t rows, uint32_t max_views,
+                   int* kernel_out, float* ms_out)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!pmats || !kernel_out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "pmats or kernel_out is NULL");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, n_views, n_modules, channels, rows);
+    if (r)
+        return r;
+    VolumeEntry* v = find_volume(ctx, volume);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
+    cudaSetDevice(ctx->device);
+    const ctlcu_settings& s = *settings;
+    if (!(s.interpolate && s.interp_mode == CTLCU_INTERP_SOFTWARE && s.volume_upsampling == 1)) {
+        *kernel_out = CTLCU_KERNEL_GATHER;  // only the gather loop serves these settings
+        return CTLCU_OK;
+    }
+    // an evenly spaced subset of the views
+    const size_t per_view = (size_t)n_modules * 12;
+    std::vector<double> hp((size_t)n_views * per_view);
+    if (is_device_ptr(pmats))
+        CU_TRY(ctx, cudaMemcpy(hp.data(), pmats, hp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    else
+        std::memcpy(hp.data(), pmats, hp.size() * sizeof(double));
+    const uint32_t nv = std::min<uint32_t>(max_views ? max_views : 8, n_views);
+    std::vector<double> sub((size_t)nv * per_view);
+    for (uint32_t i = 0; i < nv; ++i) {
+        const uint32_t src = nv == 1 ? 0 : (uint32_t)std::llround((double)i * (n_views - 1) / (nv - 1));
+        std::memcpy(&sub[i * per_view], &hp[src * per_view], per_view * sizeof(double));
+    }
+    double* d_pm = nullptr;
+    float* d_out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const int cand[3] = { CTLCU_KERNEL_CELLS, CTLCU_KERNEL_PAIRS, CTLCU_KERNEL_GATHER };
+    float ms[3] = { 0.f, 0.f, 0.f };
+    auto cleanup = [&]() {
+        cudaFree(d_pm);
+        cudaFree(d_out);
+        if (e0)
+            cudaEventDestroy(e0);
+        if (e1)
+            cudaEventDestroy(e1);
+    };
+    if (cudaMalloc(&d_pm, sub.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_out, (size_t)nv * n_modules * rows * channels * sizeof(float)) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+        cudaMemcpy(d_pm, sub.data(), sub.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cleanup();
+        return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY, "autotune scratch allocation failed");
+    }
+    for (int c = 0; c < 3 && r == CTLCU_OK; ++c) {
+        ctlcu_settings t = s;
+        t.kernel = cand[c];
+        // first run builds the variant's array and warms the caches
+        r = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
+        if (r)
+            break;
+        cudaEventRecord(e0, ctx->stream);
+        for (int k = 0; k < 3 && r == CTLCU_OK; ++k)
+            r = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            r = fail(ctx, CTLCU_ERR_CUDA, "autotune run failed");
+            break;
+        }
+        cudaEventElapsedTime(&ms[c], e0, e1);
+        ms[c] /= 3.0f;
+    }
+    cleanup();
+    if (r)
+        return r;
+    int best = 0;
+    for (int c = 1; c < 3; ++c)
+        if (ms[c] < ms[best])
+            best = c;
+    ctx->tuned[std::make_tuple(volume, channels, rows, n_modules)] = cand[best];
+    // keep only the array the chosen loop reads
+    cudaStreamSynchronize(ctx->stream);
+    if (cand[best] != CTLCU_KERNEL_CELLS && v->cells) {
+        cudaFree(v->cells);
+        ctx->used -= std::min<uint64_t>(ctx->used, v->cell_bytes);
+        v->cells = nullptr;
+        v->cell_bytes = 0;
+    }
+    if (cand[best] != CTLCU_KERNEL_PAIRS && v->pairs) {
+        cudaFree(v->pairs);
+        ctx->used -= std::min<uint64_t>(ctx->used, v->pair_bytes);
+        v->pairs = nullptr;
+        v->pair_bytes = 0;
+    }
+    *kernel_out = cand[best];
+    if (ms_out)
+        for (int c = 0; c < 3; ++c)
+            ms_out[c] = ms[c];
     return read_flags(ctx);
 }
 

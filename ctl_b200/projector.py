@@ -396,6 +396,20 @@ class Context:
                                                  C.byref(n)))
         return int(n.value)
 
+    def autotune(self, volume: Volume, pmats, channels: int, rows: int,
+                 settings: Optional[Settings] = None, max_views: int = 8):
+        """Time the sample loops on a view subset; later KERNEL_AUTO calls with this
+        volume and detector use the fastest.  Returns (kernel, {name: ms})."""
+        settings = settings or Settings()
+        P = _contig_f64(pmats)
+        k = C.c_int(0)
+        ms = (C.c_float * 3)()
+        st = settings.to_c()
+        self._check(self.lib.ctlcu_autotune(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(P)),
+                                            int(P.shape[0]), int(P.shape[1]), int(channels), int(rows),
+                                            int(max_views), C.byref(k), ms))
+        return int(k.value), {"cells": ms[0], "pairs": ms[1], "gather": ms[2]}
+
     def view_setup(self, pmats):
         P = np.ascontiguousarray(pmats, dtype=np.float64)
         V, M = P.shape[0], P.shape[1]

@@ -95,9 +95,13 @@ class DRRServer:
         V, M = req.pmats.shape[:2]
         return int(V * M * (self.rows * self.channels * 4 + 96))
 
-    def warm_up(self) -> None:
-        """Build every volume's cell array and the kernels' first launch outside timing."""
+    def warm_up(self, typical_pmats: Optional[np.ndarray] = None) -> None:
+        """Autotune the sample loop of every volume on a typical request geometry
+        (if given), build the arrays it reads and launch once, outside timing."""
         torch = self.torch
+        if typical_pmats is not None:
+            self.tuned = [self.ctx.autotune(v, typical_pmats, self.channels, self.rows, self.settings)
+                          for v in self.volumes]
         P = np.zeros((1, 1, 3, 4))
         P[0, 0, :, :3] = np.eye(3)
         P[0, 0, 2, 3] = 1000.0

@@ -199,6 +199,19 @@ CTLCU_API int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_s
                         const double* pmats, uint32_t n_views, uint32_t n_modules,
                         uint32_t channels, uint32_t rows, uint64_t* samples);
 
+/*
+ * Autotuner: times the sample loops that serve these settings (cell, pair and
+ * gather loops for software trilinear interpolation without up-sampling) on
+ * up to `max_views` evenly spaced views of the job (0 = 8), remembers the
+ * fastest for later CTLCU_KERNEL_AUTO calls on this volume with the same
+ * detector size and module count, keeps only the derived array the winner
+ * reads, and returns it in *kernel.  ms_out (optional) receives the three
+ * mean times in ms (cells, pairs, gather).  pmats: host or device.
+ */
+CTLCU_API int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                             const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,
+                             uint32_t rows, uint32_t max_views, int* kernel, float* ms_out);
+
 /* Per-(view, module) packed QR (15 doubles: Q row-major, R00 R01 R02 R11 R12 R22)
  * and per-view source position (3 doubles), computed by the device setup
  * kernel; the reference's decomposeM / determineSource

@@ -306,3 +306,18 @@ def test_batch_outside_cell_kernel_falls_back_per_request(ctx):
         want, _ = oracle.project_fp64(vol, (vox,) * 3, P, C, R, interpolate=False)
         assert rel_err(out.cpu().numpy(), want).max() <= TOL
         v.release()
+
+
+def test_autotune_chooses_and_auto_follows(ctx):
+    m, vol, P, _ = golden_cases()[0]
+    v = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]))
+    kernel, ms = ctx.autotune(v, P, m["channels"], m["rows"], Settings())
+    assert kernel in (L.KERNEL_CELLS, L.KERNEL_PAIRS, L.KERNEL_GATHER)
+    assert all(t > 0 for t in ms.values())
+    got = ctx.project(v, P, m["channels"], m["rows"], Settings())
+    want, _ = _oracle(m, vol, P)
+    assert rel_err(got, want).max() <= TOL
+    # settings outside the fast loops: only the gather loop applies
+    k2, _ = ctx.autotune(v, P, m["channels"], m["rows"], Settings(interpolate=False))
+    assert k2 == L.KERNEL_GATHER
+    v.release()
