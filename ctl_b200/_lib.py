@@ -25,6 +25,10 @@ F32, BF16, F16 = 0, 1, 2
 INTERP_SOFTWARE, INTERP_TEXTURE = 0, 1
 ACCUM_FP64, ACCUM_KAHAN, ACCUM_FP32 = 0, 1, 2
 KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS, KERNEL_PAIRS = 0, 1, 2, 3
+# cudaStreamLegacy: the handle of the legacy default stream.  A NULL stream
+# argument means the context's own (non-blocking) stream, so work ordered on
+# the default stream (torch's default) must name it with this handle.
+STREAM_LEGACY = 1
 
 STATUS_NAMES = {
     OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",

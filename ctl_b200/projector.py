@@ -64,6 +64,13 @@ def _is_cuda(x) -> bool:
     return _is_torch(x) and x.is_cuda
 
 
+def torch_stream_handle(stream) -> int:
+    """The C-ABI stream argument for a torch CUDA stream.  torch's default
+    stream has the handle 0, which the C ABI reads as the context's own
+    stream; it is passed as the legacy default stream instead."""
+    return stream.cuda_stream or L.STREAM_LEGACY
+
+
 # ---------------------------------------------------------------------------------------------
 # settings, volumes, projection data
 # ---------------------------------------------------------------------------------------------
@@ -318,7 +325,7 @@ class Context:
         for t in arrays:
             if _is_cuda(t):
                 import torch
-                return torch.cuda.current_stream(t.device).cuda_stream
+                return torch_stream_handle(torch.cuda.current_stream(t.device))
         return 0
 
     def project(self, volume: Volume, pmats, channels: int, rows: int,

@@ -29,7 +29,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from .projector import Context, Settings, Volume
+from .projector import Context, Settings, Volume, torch_stream_handle
 
 
 @dataclass
@@ -109,7 +109,7 @@ class DRRServer:
         # until the stream is synchronised, and run on torch's current stream
         # so its caching allocator orders any reuse after our kernels
         keep = []
-        stream = torch.cuda.current_stream().cuda_stream
+        stream = torch_stream_handle(torch.cuda.current_stream())
         for v in self.volumes:
             out = torch.empty((1, 1, self.rows, self.channels), device="cuda")
             dP = torch.from_numpy(P).cuda()
@@ -172,7 +172,7 @@ class DRRServer:
                             at += V * M
                             r.out = torch.empty((V, M, self.rows, self.channels), device="cuda")
                             items.append((self.volumes[r.volume], dP, r.out))
-                        self.ctx.project_batch(items, self.settings, stream=s.cuda_stream)
+                        self.ctx.project_batch(items, self.settings, stream=torch_stream_handle(s))
                         ev = torch.cuda.Event(enable_timing=True)
                         ev.record(s)
                     inflight[i] = (batch, ev)

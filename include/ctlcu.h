@@ -149,9 +149,10 @@ CTLCU_API int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* byte
  * RayCasterProjector::project (raycasterprojector.cpp:139-375) for a resident
  * volume: all n_views*n_modules matrices in one launch.
  * pmats and out may each be host or device memory.  With both on the device
- * the call is asynchronous on `stream` (NULL = the context's stream); with
- * either on the host the call copies on the context's stream and returns when
- * `out` is complete.
+ * the call is asynchronous on `stream` (NULL = the context's stream, which is
+ * non-blocking: pass cudaStreamLegacy to order the call on the legacy default
+ * stream); with either on the host the call copies on the context's stream
+ * and returns when `out` is complete.
  */
 CTLCU_API int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
                   const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,

@@ -127,6 +127,24 @@ def test_resident_device_and_host_paths_agree_bitwise(ctx):
     v.release()
 
 
+def test_device_call_is_ordered_on_torchs_current_stream(ctx):
+    """Without an explicit stream, a device-tensor call runs on torch's current
+    stream (the default stream included), so a torch read-back that follows it
+    sees the finished projections without any ctlcu_sync."""
+    import torch
+    vol = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=2)
+    P = _c2_geometry()[:32]
+    v = ctx.volume(VoxelVolume(vol, (1, 1, 1)))
+    want = ctx.project(v, P, 512, 512, Settings(kernel=L.KERNEL_GATHER))  # host pmats: synchronous
+    dP = torch.from_numpy(np.ascontiguousarray(P)).cuda()
+    torch.cuda.synchronize()
+    for stream in (torch.cuda.default_stream(), torch.cuda.Stream()):
+        with torch.cuda.stream(stream):
+            got = ctx.project(v, dP, 512, 512, Settings(kernel=L.KERNEL_GATHER)).cpu().numpy()
+        np.testing.assert_array_equal(got, want)
+    v.release()
+
+
 def test_batch_equals_individual_calls(ctx):
     import torch
     cases = golden_cases()
