@@ -29,6 +29,7 @@ KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS, KERNEL_PAIRS = 0, 1, 2, 3
 # argument means the context's own (non-blocking) stream, so work ordered on
 # the default stream (torch's default) must name it with this handle.
 STREAM_LEGACY = 1
+NOALLOC_MAX_VIEW_MODULES = 4096  # scratch entries of ctlcu_project_noalloc
 
 STATUS_NAMES = {
     OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",
@@ -70,6 +71,8 @@ SIGNATURES = [
     ("ctlcu_volume_bytes", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ctlcu_project", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                 C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("ctlcu_project_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
+                                        C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("ctlcu_project_volume", C.c_int, [C.c_void_p, C.POINTER(VolumeDesc), C.c_void_p, C.POINTER(Settings),
                                        C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                        C.c_void_p]),

@@ -704,6 +704,53 @@ void free_batch(BatchDevice& bd, cudaStream_t st, bool pooled)
     bd = BatchDevice{};
 }
 
+// ---- no-allocation projection ---------------------------------------------------------------
+
+// Geometry scratch of ctlcu_project_noalloc, in static device memory.  Host
+// code must not pass `g_noalloc_geom` itself to a kernel (on the host it names
+// a stand-in, not device memory): it uses the address that cudaGetSymbolAddress
+// returns, looked up once per device.
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) ViewGeom g_noalloc_geom[CTLCU_NOALLOC_MAX_VIEW_MODULES];
+std::mutex g_noalloc_mu;
+ViewGeom* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the context's device, which is current.
+int noalloc_scratch(ctlcu_ctx* ctx, ViewGeom** out)
+{
+    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "device ordinal %d is above the no-allocation limit %d",
+                    ctx->device, kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_geom);
+        if (e != cudaSuccess || !p)
+            return fail(ctx, CTLCU_ERR_CUDA, "address of the no-allocation scratch array: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[ctx->device] = (ViewGeom*)p;
+    }
+    *out = g_noalloc_ptr[ctx->device];
+    return CTLCU_OK;
+}
+
+// The derived array that volume_args would have to build for these (resolved)
+// settings, or nullptr when every array they read exists already.
+const char* missing_array(const VolumeEntry& v, const ctlcu_settings* s)
+{
+    const bool interp = s->interpolate != 0;
+    const int f = interp ? (int)s->volume_upsampling : 1;
+    if (f == 0 && !v.mean)
+        return "mean-voxel volume (volume_upsampling 0)";
+    if (interp && s->interp_mode == CTLCU_INTERP_TEXTURE)
+        return v.tex.count(f) ? nullptr : "interpolation texture";
+    if (interp && f == 1 && s->kernel == CTLCU_KERNEL_PAIRS)
+        return v.pairs ? nullptr : "pair array";
+    if (interp && f == 1 && s->kernel != CTLCU_KERNEL_GATHER)
+        return v.cells ? nullptr : "cell array";
+    return nullptr;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1288,6 +1335,67 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
     *launches = ctx->launches;
+    return CTLCU_OK;
+}
+
+// ctlcu_project with device pmats/out whose setup writes the ray geometry into
+// the static scratch array instead of pool memory.  Nothing has to be cleared
+// first: the setup kernel writes every (view, module) entry that the
+// projection then reads, and the flag word is zero between calls (read_flags
+// clears it).
+int ctlcu_project_noalloc(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                          const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,
+                          uint32_t rows, float* out, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!pmats || !out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "pmats or out is NULL");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, n_views, n_modules, channels, rows);
+    if (r)
+        return r;
+    const uint64_t nvm = (uint64_t)n_views * n_modules;
+    if (nvm > CTLCU_NOALLOC_MAX_VIEW_MODULES)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "%llu view-modules exceed the no-allocation scratch limit of %d; split the call",
+                    (unsigned long long)nvm, CTLCU_NOALLOC_MAX_VIEW_MODULES);
+    VolumeEntry* v = find_volume(ctx, volume);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
+    cudaSetDevice(ctx->device);
+    if (!is_device_ptr(pmats) || !is_device_ptr(out))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "the no-allocation call needs device pmats and out (host buffers need staging memory)");
+    const ctlcu_settings eff = resolve_kernel(ctx, *v, settings, channels, rows, n_modules);
+    if (const char* what = missing_array(*v, &eff))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "the %s of this volume is not built; project it once with ctlcu_project first", what);
+    ViewGeom* geom = nullptr;
+    r = noalloc_scratch(ctx, &geom);
+    if (r)
+        return r;
+    ProjectArgs a = {};
+    Mode mode;
+    int dtype;
+    r = volume_args(ctx, *v, &eff, a, mode, dtype);
+    if (r)
+        return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    r = order_after_staging(ctx, st);
+    if (r)
+        return r;
+    job_args(a, &eff, n_views, n_modules, channels, rows);
+    CU_TRY(ctx, launch_setup(pmats, n_views, n_modules, geom, nullptr, nullptr, ctx->d_flags, st));
+    a.geom = geom;
+    a.out = out;
+    a.flags = ctx->d_flags;
+    a.counter = nullptr;
+    CU_TRY(ctx, launch_project(a, mode, (Accum)eff.accum, dtype, st));
+    ctx->launches += 2;
     return CTLCU_OK;
 }
 

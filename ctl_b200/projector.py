@@ -342,6 +342,21 @@ class Context:
                                            C.c_void_p(stream or None)))
         return out
 
+    def project_noalloc(self, volume: Volume, pmats, out, settings: Optional[Settings] = None,
+                        stream: int = 0):
+        """ctlcu_project_noalloc, for callers that cannot allocate device memory
+        during the call: device pmats (V,M,3,4) f64 and out (V,M,R,C) f32; the
+        ray geometry goes into the library's static scratch array (at most
+        NOALLOC_MAX_VIEW_MODULES view-modules per call)."""
+        settings = settings or Settings()
+        V, M = int(pmats.shape[0]), int(pmats.shape[1])
+        R, Ch = int(out.shape[2]), int(out.shape[3])
+        st = settings.to_c()
+        stream = self._stream_for(stream, pmats, out)
+        self._check(self.lib.ctlcu_project_noalloc(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(pmats)),
+                                                   V, M, Ch, R, C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
+        return out
+
     def project_volume(self, vol: VoxelVolume, pmats, channels: int, rows: int,
                        settings: Optional[Settings] = None, out=None):
         """One-shot: upload, project, release (the reference's per-call semantics)."""

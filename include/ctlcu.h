@@ -223,6 +223,35 @@ CTLCU_API int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_v
 /* Number of kernels this library has launched on the context (all calls). */
 CTLCU_API int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches);
 
+/*
+ * No counterpart in the reference.  ctlcu_project for callers that cannot
+ * allocate device memory while they run: a real-time loop that reserved all
+ * of its memory up front, or a host whose allocator must not be entered
+ * (an allocation can synchronise the device or fail when memory is full).
+ * This call makes no device allocation.  The per-(view, module) ray geometry
+ * goes into one fixed scratch array in the library's static device memory:
+ * CTLCU_NOALLOC_MAX_VIEW_MODULES entries of 104 bytes (416 KiB), held on every
+ * device that loads the library until the process exits.  A call with more
+ * than that many view-modules (n_views * n_modules) fails with
+ * CTLCU_ERR_INVALID_ARGUMENT; split it.
+ *  - pmats and out must be device memory (host buffers would need staging
+ *    memory); asynchronous on `stream` as ctlcu_project; singular matrices
+ *    are reported by ctlcu_sync.
+ *  - Every derived array the settings read (the cell or pair array, the
+ *    mean-voxel volume, a texture) must exist already, built by an earlier
+ *    ctlcu_project or ctlcu_autotune of this volume with these settings;
+ *    otherwise CTLCU_ERR_INVALID_ARGUMENT names the missing one.
+ *  - The first call on a device looks up the scratch array's address there
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - Every call on a device shares the one scratch array: calls whose work
+ *    overlaps on the GPU (on different streams or contexts) race on it, so
+ *    serialise them (one stream, or events between them).
+ */
+#define CTLCU_NOALLOC_MAX_VIEW_MODULES 4096
+CTLCU_API int ctlcu_project_noalloc(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                                    const double* pmats, uint32_t n_views, uint32_t n_modules,
+                                    uint32_t channels, uint32_t rows, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
