@@ -216,6 +216,41 @@ def test_c2_full_size_views_match_oracle(ctx):
     v.release()
 
 
+@pytest.mark.parametrize("storage,deq", [(L.BF16, dequant_bf16), (L.F16, dequant_f16)], ids=["bf16", "f16"])
+def test_c2_full_size_16bit_storage_matches_dequantised_oracle(ctx, storage, deq):
+    """256^3 -> 512^2 with the volume stored in 16 bits: the cell, pair and
+    gather loops against the oracle on the dequantised volume."""
+    vol = Ph.ellipsoid_phantom((256, 256, 256), (1, 1, 1), 40, seed=2)
+    P = _c2_geometry()[[0, 181]]
+    v = ctx.volume(VoxelVolume(vol, (1, 1, 1)), storage)
+    want, _ = oracle.project_fp64(deq(vol), (1, 1, 1), P, 512, 512)
+    for kernel in (L.KERNEL_CELLS, L.KERNEL_PAIRS, L.KERNEL_GATHER):
+        gpu = ctx.project(v, P, 512, 512, Settings(kernel=kernel))
+        e = rel_err(gpu, want)
+        assert e.max() <= TOL, (kernel, e.max())
+    v.release()
+
+
+def test_batch_mixing_storage_types_matches_single_calls(ctx):
+    """One persistent launch over volumes stored as FP32 and BF16 gives each
+    request the result of its own single call."""
+    import torch
+    m, vol, P, _ = golden_cases()[0]
+    vf = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]), L.F32)
+    vb = ctx.volume(VoxelVolume(vol, m["voxel"], m["offset"]), L.BF16)
+    for kernel in (L.KERNEL_CELLS, L.KERNEL_PAIRS):
+        s = _settings(m, kernel=kernel)
+        dP = torch.from_numpy(np.ascontiguousarray(P)).cuda()
+        outs = [torch.empty((P.shape[0], P.shape[1], m["rows"], m["channels"]), device="cuda") for _ in range(2)]
+        ctx.project_batch([(vf, dP, outs[0]), (vb, dP, outs[1])], s)
+        torch.cuda.synchronize()
+        ctx.sync()
+        for v, o in ((vf, outs[0]), (vb, outs[1])):
+            np.testing.assert_array_equal(o.cpu().numpy(), ctx.project(v, P, m["channels"], m["rows"], s))
+    vf.release()
+    vb.release()
+
+
 def test_cells_kernel_rejects_unsupported_settings(ctx):
     m, vol, P, _ = golden_cases()[0]
     for bad in (dict(interpolate=False), dict(volume_upsampling=2), dict(interp_mode=L.INTERP_TEXTURE)):
