@@ -47,6 +47,9 @@ CHANNELS = ROWS = 512
 N_VIEWS = 360
 METRIC = "projections/s at 256^3->512^2 (plain FP32)"
 WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
+# DRAM bytes (read + write) of one 360-view launch of the cell loop on this
+# workload, from one ncu capture (profiles/project_kernel_cells_256cubed_to_512sq_dram.md)
+CELLS_TRAFFIC_BYTES = 7.90e9 + 0.75271e9
 
 
 def make_inputs(n_views: int = N_VIEWS):
@@ -251,10 +254,10 @@ def run_ours(args):
     ms_per_step = total_ms / args.steps
     value = world * n_views * args.steps / (total_ms / 1e3)
 
-    # the projection kernel alone: each step is one setup launch + one projection launch;
-    # time a setup-only run to split them
-    from ctl_b200.projector import Context as _C  # noqa: F401
-    kernel_ms = ms_per_step  # refined below when the profile split is known
+    # Each step is one setup launch (about 5 us for 360 views) and one projection
+    # launch, timed together by the events on their stream; the step time stands
+    # for the projection kernel's launch time (the setup is < 0.01% of it).
+    kernel_ms = ms_per_step
 
     # e2e through the C ABI with host buffers (pinned)
     h_vol = torch.from_numpy(vol).pin_memory()
@@ -282,6 +285,9 @@ def run_ours(args):
         mhz = clk.get("sm_mhz") or 1965.0
         l1_peak = sms * 128 * mhz * 1e6 / 1e9  # GB/s
         achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+        loop = tuned[0] if tuned is not None else settings.kernel
+        traffic = (CELLS_TRAFFIC_BYTES if loop == L.KERNEL_CELLS and n_views == N_VIEWS and
+                   settings.storage == L.F32 and settings.interp_mode == L.INTERP_SOFTWARE else None)
         line = {
             "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -304,7 +310,9 @@ def run_ours(args):
                 "chosen": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs", L.KERNEL_GATHER: "gather"}[tuned[0]],
                 "ms_on_8_views": tuned[1]},
             "roofline": {"bound": "l1", "achieved": achieved, "peak": l1_peak, "unit": "GB/s",
-                         "frac": achieved / l1_peak, "traffic": None,
+                         "frac": achieved / l1_peak, "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch"
+                                           if traffic else "not captured for this variant",
                          "peak_source": f"{sms} SMs x 128 B/clk x {mhz:.0f} MHz sampled SM clock",
                          "algorithmic_bytes_per_launch": alg_bytes},
             "clocks": clk,

@@ -3,7 +3,9 @@
 
 #include <QDebug>
 #include <algorithm>
+#include <cmath>
 #include <stdexcept>
+#include <string>
 
 namespace CTL {
 namespace CUDA {
