@@ -49,6 +49,25 @@ class Settings(C.Structure):
                 ("interp_mode", C.c_int32), ("accum", C.c_int32), ("kernel", C.c_int32)]
 
 
+TRAJ_HELICAL, TRAJ_AXIAL, TRAJ_WOBBLE, TRAJ_SHORT_SCAN, TRAJ_CIRCLE_PLUS_LINE = 0, 1, 2, 3, 4
+
+
+class DetectorDesc(C.Structure):
+    _fields_ = [("pixels", C.c_uint32 * 2), ("pixel_mm", C.c_double * 2), ("n_modules", C.c_uint32),
+                ("flat_panel", C.c_int32), ("angulation_rad", C.c_double), ("module_spacing_mm", C.c_double),
+                ("skew", C.c_double)]
+
+
+class TrajectoryDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32),
+                ("sdd_mm", C.c_double), ("sid_mm", C.c_double), ("pitch_mm", C.c_double), ("tilt_rad", C.c_double),
+                ("angle_increment_rad", C.c_double), ("pitch_increment_mm", C.c_double),
+                ("start_pitch_mm", C.c_double), ("start_angle_rad", C.c_double),
+                ("carm_span_mm", C.c_double), ("source_to_iso_mm", C.c_double), ("angle_span_rad", C.c_double),
+                ("wobble_angle_rad", C.c_double), ("wobble_freq", C.c_double),
+                ("line_length_mm", C.c_double), ("line_fraction", C.c_double)]
+
+
 class Request(C.Structure):
     _fields_ = [("volume", C.c_uint64), ("pmats", C.c_void_p), ("out", C.c_void_p),
                 ("n_views", C.c_uint32), ("n_modules", C.c_uint32), ("channels", C.c_uint32),
@@ -91,6 +110,8 @@ SIGNATURES = [
     ("ctlcu_view_setup", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                    C.c_void_p]),
     ("ctlcu_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("ctlcu_encode_geometry", C.c_int, [C.c_void_p, C.POINTER(DetectorDesc), C.POINTER(TrajectoryDesc), C.c_uint32,
+                                        C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

@@ -1338,6 +1338,60 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
     return CTLCU_OK;
 }
 
+int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
+                          const ctlcu_trajectory_desc* trajectory, uint32_t n_views, double* pmats, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!detector || !trajectory || !pmats)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "detector, trajectory or pmats is NULL");
+    const ctlcu_detector_desc& d = *detector;
+    const ctlcu_trajectory_desc& t = *trajectory;
+    if (n_views == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "n_views is 0");
+    if (d.pixels[0] == 0 || d.pixels[1] == 0 || !(d.pixel_mm[0] > 0.0) || !(d.pixel_mm[1] > 0.0))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "detector pixel counts and sizes must be positive");
+    if (d.n_modules == 0 || (d.flat_panel && d.n_modules != 1))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "a detector has >= 1 modules, a flat panel exactly 1");
+    if (!d.flat_panel && std::fabs(d.angulation_rad) <= 1e-12 && d.n_modules > 1)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                    "a cylindrical detector of several modules needs a nonzero angulation");
+    if (!std::isfinite(d.angulation_rad) || !std::isfinite(d.module_spacing_mm) || !std::isfinite(d.skew))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "detector parameters must be finite");
+    const bool tubular = t.kind == CTLCU_TRAJ_HELICAL || t.kind == CTLCU_TRAJ_AXIAL;
+    const bool carm = t.kind == CTLCU_TRAJ_WOBBLE || t.kind == CTLCU_TRAJ_SHORT_SCAN ||
+                      t.kind == CTLCU_TRAJ_CIRCLE_PLUS_LINE;
+    if (!tubular && !carm)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown trajectory kind %d", t.kind);
+    if (tubular && !(t.sdd_mm > 0.0 && t.sid_mm > 0.0))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "a tubular gantry needs positive SDD and SID");
+    if (carm && !(t.carm_span_mm > 0.0))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "a C-arm gantry needs a positive C-arm span");
+    if (t.kind == CTLCU_TRAJ_CIRCLE_PLUS_LINE && !(t.line_fraction >= 0.0 && t.line_fraction <= 1.0))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "line_fraction must lie in [0, 1]");
+    const uint64_t n = (uint64_t)n_views * d.n_modules;
+    if (n > 0x7fffffffull)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many matrices");
+    cudaSetDevice(ctx->device);
+    const bool dev = is_device_ptr(pmats);
+    cudaStream_t st = dev && stream ? (cudaStream_t)stream : ctx->stream;
+    double* out = pmats;
+    if (!dev)
+        CU_TRY(ctx, cudaMallocAsync((void**)&out, n * 12 * sizeof(double), st));
+    cudaError_t e = launch_encode_geometry(d, t, n_views, out, st);
+    if (e == cudaSuccess && !dev)
+        e = cudaMemcpyAsync(pmats, out, n * 12 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (!dev)
+        cudaFreeAsync(out, st);
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "geometry encoding: %s", cudaGetErrorString(e));
+    ++ctx->launches;
+    if (!dev)
+        CU_TRY(ctx, cudaStreamSynchronize(st));
+    return CTLCU_OK;
+}
+
 // ctlcu_project with device pmats/out whose setup writes the ray geometry into
 // the static scratch array instead of pool memory.  Nothing has to be cleared
 // first: the setup kernel writes every (view, module) entry that the

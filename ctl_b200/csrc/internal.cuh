@@ -1,6 +1,8 @@
 // Internal types shared by the ctlcu translation units.
 #pragma once
 
+#include "ctlcu.h"
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -232,5 +234,7 @@ cudaError_t launch_build_pairs(const void* padded, const int n[3], int dtype, co
                                void* pairs, cudaStream_t s);
 cudaError_t launch_unpad_upsample(const void* padded, const int n[3], int dtype, int f, void* dst,
                                   cudaStream_t s);
+cudaError_t launch_encode_geometry(const ctlcu_detector_desc& det, const ctlcu_trajectory_desc& traj,
+                                   uint32_t n_views, double* pmats, cudaStream_t s);
 
 }  // namespace ctlcu

@@ -273,6 +273,7 @@ struct CellCache {
     float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f;
 };
 
+#if CTLCU_CELL_PREFETCH > 0
 // Cell index of the sample at step kk (the cell layout makes the magic
 // offsets cancel, see CellLayout), clamped to the array.
 __device__ __forceinline__ uint32_t cell_index(float2 kk, float2 bxy, float bz, float2 dxy, float dz,
@@ -283,6 +284,7 @@ __device__ __forceinline__ uint32_t cell_index(float2 kk, float2 bxy, float bz, 
     const uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
     return min(idx, cmax);
 }
+#endif
 
 __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const char* __restrict__ cells, float2 kk,
                                              float2 bxy,

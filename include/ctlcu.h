@@ -223,6 +223,59 @@ CTLCU_API int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_v
 /* Number of kernels this library has launched on the context (all calls). */
 CTLCU_API int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches);
 
+/* ---- geometry encoding ------------------------------------------------------------------- */
+
+/* Detector of a simple CT system: CylindricalDetector(nbPixelPerModule,
+ * pixelDimensions, nbDetectorModules, angulationPerModule, moduleSpacing)
+ * (components/cylindricaldetector.h) or, with flat_panel = 1 and one module,
+ * FlatPanelDetector (components/flatpaneldetector.h).  skew: the detector's
+ * skewCoefficient (0 in CTL's stock detectors). */
+typedef struct {
+    uint32_t pixels[2];        /* channels, rows per module */
+    double pixel_mm[2];        /* pixel width, height */
+    uint32_t n_modules;
+    int32_t flat_panel;
+    double angulation_rad;     /* per module */
+    double module_spacing_mm;
+    double skew;
+} ctlcu_detector_desc;
+
+/* The stock acquisition protocols of acquisition/trajectories.h with their gantry. */
+typedef enum {
+    CTLCU_TRAJ_HELICAL = 0,          /* HelicalTrajectory on a TubularGantry */
+    CTLCU_TRAJ_AXIAL = 1,            /* AxialScanTrajectory on a TubularGantry */
+    CTLCU_TRAJ_WOBBLE = 2,           /* WobbleTrajectory on a CarmGantry */
+    CTLCU_TRAJ_SHORT_SCAN = 3,       /* ShortScanTrajectory on a CarmGantry */
+    CTLCU_TRAJ_CIRCLE_PLUS_LINE = 4  /* CirclePlusLineTrajectory on a CarmGantry */
+} ctlcu_trajectory_kind;
+
+typedef struct {
+    int32_t kind;                 /* ctlcu_trajectory_kind */
+    int32_t reserved;
+    /* TubularGantry(sourceToDetectorDistance, sourceToIsoCenterDistance, -, pitchPosition, tiltAngle) */
+    double sdd_mm, sid_mm, pitch_mm, tilt_rad;
+    /* HelicalTrajectory(angleIncrement, pitchIncrement, startPitch, startAngle); startAngle
+     * is shared with the axial and C-arm protocols */
+    double angle_increment_rad, pitch_increment_mm, start_pitch_mm, start_angle_rad;
+    /* CarmGantry(cArmSpan) and the C-arm protocols' sourceToIsocenter, angleSpan (a negative
+     * short-scan span selects 180 deg + fan angle), wobbleAngle, wobbleFreq, lineLength,
+     * fractionOfViewsForLine */
+    double carm_span_mm, source_to_iso_mm, angle_span_rad, wobble_angle_rad, wobble_freq;
+    double line_length_mm, line_fraction;
+} ctlcu_trajectory_desc;
+
+/*
+ * GeometryEncoder::encodeFullGeometry (acquisition/geometryencoder.cpp:67-117)
+ * for a simple system of the detector above on the trajectory's gantry:
+ * n_views x n_modules normalised projection matrices, [view][module] 3x4
+ * row-major, FP64, computed on the device in one launch.  pmats: device memory
+ * (asynchronous on `stream`, NULL = the context's stream) or host memory
+ * (returns when the matrices are written).
+ */
+CTLCU_API int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
+                                    const ctlcu_trajectory_desc* trajectory, uint32_t n_views, double* pmats,
+                                    void* stream);
+
 /*
  * No counterpart in the reference.  ctlcu_project for callers that cannot
  * allocate device memory while they run: a real-time loop that reserved all

@@ -51,6 +51,29 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(L.Request) == 8 + 8 + 8 + 4 * 4
 
 
+def test_struct_layouts_match_a_c_compiler(tmp_path):
+    """sizeof and field offsets of every header struct, as gcc lays them out,
+    against the ctypes binding."""
+    structs = {"ctlcu_volume_desc": L.VolumeDesc, "ctlcu_settings": L.Settings, "ctlcu_request": L.Request,
+               "ctlcu_detector_desc": L.DetectorDesc, "ctlcu_trajectory_desc": L.TrajectoryDesc}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ctlcu.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                               check=True).stdout.splitlines())
+    for cname, cls in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, (cname, fname)
+
+
 def test_default_settings_are_the_reference_defaults():
     s = L.load().ctlcu_settings_default()
     assert list(s.rays_per_pixel) == [1, 1]
