@@ -452,6 +452,81 @@ def run_geometry(args):
     ctx.close()
 
 
+def run_postops(args):
+    """Poisson noise (PoissonNoiseExtension) on the 256^3 -> 360 x 512^2 projections, on
+    the device, against the reference's own noise engine (per-view std::mt19937_64 with
+    libstdc++'s distributions, oracle/poisson_ref.cpp) on the host."""
+    import torch
+
+    from ctl_b200.projector import Context, Settings, VoxelVolume
+    vol, P = make_inputs()
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    volume = ctx.volume(VoxelVolume(vol, VOXEL))
+    dP = torch.from_numpy(P).cuda()
+    clean = ctx.project(volume, dP, CHANNELS, ROWS, Settings(), stream=ctx.stream)
+    torch.cuda.synchronize()
+    i0 = np.array([1.0e4], np.float32)   # photons per pixel: counts from 1e4 down to single digits
+    work = torch.empty_like(clean)
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.steps):
+            work.copy_(clean)   # fresh input each step, outside the events (the noise is in place)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.poisson_noise(work, i0, SEED_NOISE + i, stream=ctx.stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                times.append(a.elapsed_time(b))
+    n = clean.numel()
+    t_ms = statistics.mean(times)
+    host = clean.cpu().numpy()
+    e2e = []
+    for i in range(max(1, args.e2e_steps)):
+        h = host.copy()
+        t0 = time.perf_counter()
+        ctx.poisson_noise(h, i0, SEED_NOISE + i)
+        e2e.append(time.perf_counter() - t0)
+    extra = {"e2e": {"value": N_VIEWS / statistics.mean(e2e), "unit": "projections/s",
+                     "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes),
+                     "path": "ctlcu_poisson_noise on host data"},
+             "gpu_launches": 1,
+             "pixels_per_step": int(n),
+             "roofline": {"bound": "hbm", "achieved": 8.0 * n / (t_ms / 1e3) / 1e9, "peak": hbm_peak(),
+                          "unit": "GB/s", "frac": 8.0 * n / (t_ms / 1e3) / 1e9 / hbm_peak(),
+                          "algorithmic_bytes_per_launch": int(8 * n),
+                          "note": "4 B read + 4 B write per pixel; the FP64 sampler (PTRS with lgamma) "
+                                  "is the actual limit, not HBM"}}
+    if not args.no_cpu_baseline:
+        import oracle
+        sample = 4
+        x = host[:sample].copy()
+        t0 = time.perf_counter()
+        oracle.poisson_noise_reference(x, i0, SEED_NOISE)
+        dt = time.perf_counter() - t0
+        extra["cpu_baseline"] = {"value": sample / dt, "unit": "projections/s", "cores": 1, "kind": "port",
+                                 "sample": f"{sample} of {N_VIEWS} views with the reference's per-view "
+                                           f"mt19937_64 + std:: distributions, {dt:.2f} s"}
+    _line("projections/s through Poisson noise (PoissonNoiseExtension), 360 x 512^2, i0 = 1e4",
+          N_VIEWS / (t_ms / 1e3), "projections/s", t_ms, args,
+          {"workload": WORKLOAD + "; then Poisson noise, i0 = 1e4 photons/pixel"}, **extra)
+    volume.release()
+    ctx.close()
+
+
+def hbm_peak() -> float:
+    """The measured HBM copy bandwidth of this pool's B200s (GB/s), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+SEED_NOISE = 20240611
+
+
 def run_c4(args):
     """64 uneven volumes: one persistent launch replayed from a CUDA graph vs 64 sequential calls."""
     import torch
@@ -549,7 +624,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5", "geometry"], default="c2",
+    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5", "geometry", "postops"], default="c2",
                     help="c2 (default) is the headline; the others print extra lines")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
@@ -563,6 +638,8 @@ def main():
         return run_c5(args)
     if args.config == "geometry":
         return run_geometry(args)
+    if args.config == "postops":
+        return run_postops(args)
     return run_ours(args)
 
 

@@ -112,6 +112,12 @@ SIGNATURES = [
     ("ctlcu_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ctlcu_encode_geometry", C.c_int, [C.c_void_p, C.POINTER(DetectorDesc), C.POINTER(TrajectoryDesc), C.c_uint32,
                                         C.c_void_p, C.c_void_p]),
+    ("ctlcu_transform_to_extinction", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p,
+                                                C.c_void_p]),
+    ("ctlcu_transform_to_intensity", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p,
+                                               C.c_void_p]),
+    ("ctlcu_poisson_noise", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                      C.c_uint64, C.c_void_p]),
 ]
 
 _lib = None

@@ -751,6 +751,64 @@ const char* missing_array(const VolumeEntry& v, const ctlcu_settings* s)
     return nullptr;
 }
 
+// Runs op(device_data, stream) over `bytes` of float data in device or host
+// memory.  Host data is staged through pool memory on the context's stream,
+// and the call returns when the result is back in host memory.
+template <typename Op>
+int on_device_data(ctlcu_ctx* ctx, float* data, size_t bytes, void* stream, const char* what, Op op)
+{
+    const bool dev = is_device_ptr(data);
+    cudaStream_t st = dev && stream ? (cudaStream_t)stream : ctx->stream;
+    float* d = data;
+    if (!dev) {
+        CU_TRY(ctx, cudaMallocAsync((void**)&d, bytes, st));
+        CU_TRY(ctx, cudaMemcpyAsync(d, data, bytes, cudaMemcpyHostToDevice, st));
+    }
+    cudaError_t e = op(d, st);
+    if (e == cudaSuccess && !dev)
+        e = cudaMemcpyAsync(data, d, bytes, cudaMemcpyDeviceToHost, st);
+    if (!dev)
+        cudaFreeAsync(d, st);
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    ++ctx->launches;
+    if (!dev)
+        CU_TRY(ctx, cudaStreamSynchronize(st));
+    return CTLCU_OK;
+}
+
+// ctlcu_transform_to_extinction / _intensity
+int transform(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t per_view, const double* i0, void* stream,
+              bool to_extinction)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!data)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "data is NULL");
+    if (n_views == 0 || per_view == 0)
+        return CTLCU_OK;
+    if (per_view > (1ull << 40) / n_views)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many values");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(float) * per_view * n_views;
+    return on_device_data(ctx, data, bytes, stream, to_extinction ? "transform to extinction" : "transform to intensity",
+                          [&](float* d, cudaStream_t st) {
+                              double* di0 = nullptr;
+                              cudaError_t e = cudaSuccess;
+                              if (i0) {
+                                  e = cudaMallocAsync((void**)&di0, sizeof(double) * n_views, st);
+                                  if (e == cudaSuccess)
+                                      e = cudaMemcpyAsync(di0, i0, sizeof(double) * n_views, cudaMemcpyHostToDevice, st);
+                              }
+                              if (e == cudaSuccess)
+                                  e = launch_transform(d, per_view, n_views, di0, to_extinction, st);
+                              if (di0)
+                                  cudaFreeAsync(di0, st);
+                              return e;
+                          });
+}
+
 }  // namespace
 
 extern "C" {
@@ -1336,6 +1394,52 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
     std::lock_guard<std::mutex> lk(ctx->mu);
     *launches = ctx->launches;
     return CTLCU_OK;
+}
+
+int ctlcu_transform_to_extinction(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
+                                  const double* i0, void* stream)
+{
+    return transform(ctx, data, n_views, values_per_view, i0, stream, true);
+}
+
+int ctlcu_transform_to_intensity(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
+                                 const double* i0, void* stream)
+{
+    return transform(ctx, data, n_views, values_per_view, i0, stream, false);
+}
+
+int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t n_modules, uint32_t pixels_per_module,
+                        const float* i0_per_module, uint64_t seed, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!data || !i0_per_module)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "data or i0_per_module is NULL");
+    const uint64_t per_view = (uint64_t)n_modules * pixels_per_module;
+    if (n_views == 0 || per_view == 0)
+        return CTLCU_OK;
+    if (per_view > 0xffffffffull)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "more than 2^32 pixels per view");
+    // poissonnoiseextension.cpp:160: views whose i0 sum is (fuzzy) zero are skipped
+    float sum = 0.0f;
+    for (uint32_t m = 0; m < n_modules; ++m)
+        sum += i0_per_module[m];
+    if (std::fabs(sum) <= 1e-5f)
+        return CTLCU_OK;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(float) * per_view * n_views;
+    return on_device_data(ctx, data, bytes, stream, "Poisson noise", [&](float* d, cudaStream_t st) {
+        float* di0 = nullptr;
+        cudaError_t e = cudaMallocAsync((void**)&di0, sizeof(float) * n_modules, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(di0, i0_per_module, sizeof(float) * n_modules, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = launch_poisson_noise(d, n_views, n_modules, pixels_per_module, di0, seed, st);
+        if (di0)
+            cudaFreeAsync(di0, st);
+        return e;
+    });
 }
 
 int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,

@@ -1,0 +1,170 @@
+// Post-projection operations on the device: extinction <-> intensity and
+// Poisson (quantum) noise.
+//
+// Reference (modules/src/...):
+//   SingleViewData::transformToExtinction / transformToCounts (img/singleviewdata.cpp:135-172):
+//     p = log(float(i0) / p),  p = float(i0) * exp(-p); transformToIntensity is
+//     transformToCounts (img/projectiondata.cpp), with one i0 per view
+//   PoissonNoiseExtension::extendedProject / processViewCompact
+//     (projectors/poissonnoiseextension.cpp:35-68, :156-198):
+//     count = i0[module] exp(-p); noisy ~ Poisson(count) for count < 1e4, else
+//     Normal(count, sqrt(count)); p = log(i0[module] / noisy); views whose i0
+//     sum is zero are left as they are.
+//
+// The reference draws each view's noise from one sequential mt19937_64 stream
+// on the host (seed + view).  A sequential stream does not map onto a GPU, so
+// every pixel here draws from its own counter-based stream instead:
+// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC 2011), key = the 64-bit seed, counter = (pixel of the
+// view, view, draw index, 0).  The variates are exact for the same
+// distributions: inversion by sequential search for count < 10, Hormann's
+// transformed rejection with squeeze (PTRS; "The transformed rejection method
+// for generating Poisson random variables", Insurance: Mathematics and
+// Economics 12, 1993) for 10 <= count < 1e4, and Box-Muller above.  The mean
+// count is formed in FP64 (the reference: FP32), so it does not depend on the
+// last bit of an FP32 exp.
+#include "ctlcu.h"
+#include "internal.cuh"
+
+namespace ctlcu {
+
+namespace {
+
+struct Philox4 {
+    uint32_t x, y, z, w;
+};
+
+// Philox4x32 with 10 rounds; multipliers and Weyl key increments of the SC'11 paper
+__device__ __forceinline__ Philox4 philox4x32_10(Philox4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = Philox4{ (uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0 };
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// A double in (0, 1) from 53 random bits of two words
+__device__ __forceinline__ double uniform53(uint32_t a, uint32_t b)
+{
+    return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+struct Stream {
+    uint32_t pixel, view, draw, k0, k1;
+    __device__ __forceinline__ void next(double& u, double& v)
+    {
+        const Philox4 r = philox4x32_10(Philox4{ pixel, view, draw++, 0u }, k0, k1);
+        u = uniform53(r.x, r.y);
+        v = uniform53(r.z, r.w);
+    }
+};
+
+constexpr int kMaxRejections = 64;  // PTRS accepts > 85% of candidates; 64 rejections never occur
+
+// Poisson(lam) for 0 <= lam < 1e4, or Normal(lam, sqrt(lam)) for lam >= 1e4,
+// as the FP32 count the reference then takes the log of
+__device__ float noisy_count(double lam, Stream& s)
+{
+    double u, v;
+    if (!((float)lam < 1.0e4f)) {
+        s.next(u, v);
+        const double z = sqrt(-2.0 * log(u)) * cos(6.283185307179586 * v);
+        return (float)(lam + sqrt(lam) * z);
+    }
+    if (lam < 10.0) {
+        // inversion: the smallest k with F(k) >= u
+        s.next(u, v);
+        double p = exp(-lam), F = p;
+        int k = 0;
+        while (u > F && k < 1000) {
+            ++k;
+            p *= lam / k;
+            F += p;
+        }
+        return (float)k;
+    }
+    const double slam = sqrt(lam), loglam = log(lam);
+    const double b = 0.931 + 2.53 * slam;
+    const double a = -0.059 + 0.02483 * b;
+    const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < kMaxRejections; ++it) {
+        s.next(u, v);
+        const double U = u - 0.5;
+        const double us = 0.5 - fabs(U);
+        const double k = floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && v <= vr)
+            return (float)k;
+        if (k < 0.0 || (us < 0.013 && v > us))
+            continue;
+        if (log(v) + log(inv_alpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0))
+            return (float)k;
+    }
+    return (float)floor(lam + 0.5);  // unreachable in practice (probability < 1e-50)
+}
+
+__global__ void poisson_kernel(float* __restrict__ data, uint32_t n_views, uint32_t n_modules, uint32_t ppm,
+                               const float* __restrict__ i0, uint32_t k0, uint32_t k1)
+{
+    const uint64_t per_view = (uint64_t)n_modules * ppm;
+    const uint64_t total = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t view = (uint32_t)(i / per_view);
+        const uint32_t pix = (uint32_t)(i - (uint64_t)view * per_view);
+        const float i0m = i0[pix / ppm];
+        const double lam = (double)i0m * exp(-(double)data[i]);
+        Stream s{ pix, view, 0u, k0, k1 };
+        const float noisy = noisy_count(lam, s);
+        data[i] = logf(i0m / noisy);
+    }
+}
+
+__global__ void intensity_kernel(float* __restrict__ data, uint64_t per_view, uint32_t n_views,
+                                 const double* __restrict__ i0, int to_extinction)
+{
+    const uint64_t total = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float i0f = i0 ? (float)i0[i / per_view] : 1.0f;
+        const float p = data[i];
+        data[i] = to_extinction ? logf(i0f / p) : i0f * expf(-p);
+    }
+}
+
+unsigned grid_for_elements(uint64_t n)
+{
+    uint64_t b = (n + 255) / 256;
+    const uint64_t cap = 148ull * 16;  // a few waves; the loops stride over the rest
+    return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modules, uint32_t ppm, const float* i0,
+                                 uint64_t seed, cudaStream_t s)
+{
+    const uint64_t total = (uint64_t)n_views * n_modules * ppm;
+    if (total == 0)
+        return cudaSuccess;
+    poisson_kernel<<<grid_for_elements(total), 256, 0, s>>>(data, n_views, n_modules, ppm, i0, (uint32_t)seed,
+                                                             (uint32_t)(seed >> 32));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transform(float* data, uint64_t per_view, uint32_t n_views, const double* i0, bool to_extinction,
+                             cudaStream_t s)
+{
+    const uint64_t total = per_view * n_views;
+    if (total == 0)
+        return cudaSuccess;
+    intensity_kernel<<<grid_for_elements(total), 256, 0, s>>>(data, per_view, n_views, i0, to_extinction ? 1 : 0);
+    return cudaGetLastError();
+}
+
+}  // namespace ctlcu

@@ -357,6 +357,50 @@ class Context:
                                                    V, M, Ch, R, C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
         return out
 
+    @staticmethod
+    def _inplace_f32(data):
+        if _is_torch(data):
+            import torch
+            if data.dtype != torch.float32 or not data.is_contiguous():
+                raise ValueError("data must be a contiguous float32 tensor (changed in place)")
+        elif not (isinstance(data, np.ndarray) and data.dtype == np.float32 and data.flags.c_contiguous):
+            raise ValueError("data must be a C-contiguous float32 array (changed in place)")
+        return data
+
+    def _transform(self, fn, data, i0, stream):
+        data = self._inplace_f32(data)
+        V = int(data.shape[0])
+        per_view = int(np.prod(tuple(data.shape[1:]))) if data.ndim > 1 else 1
+        arr = None
+        if i0 is not None:
+            arr = np.ascontiguousarray(np.broadcast_to(np.asarray(i0, np.float64), (V,)))
+        stream = self._stream_for(stream, data)
+        self._check(fn(self.h, C.c_void_p(_ptr(data)), V, per_view,
+                       C.c_void_p(arr.ctypes.data if arr is not None else None), C.c_void_p(stream or None)))
+        return data
+
+    def transform_to_extinction(self, data, i0=None, stream: int = 0):
+        """ProjectionData::transformToExtinction: p = log(i0 / p) in place, one i0
+        per view (scalar, sequence of views, or None for 1)."""
+        return self._transform(self.lib.ctlcu_transform_to_extinction, data, i0, stream)
+
+    def transform_to_intensity(self, data, i0=None, stream: int = 0):
+        """ProjectionData::transformToIntensity: p = i0 exp(-p) in place."""
+        return self._transform(self.lib.ctlcu_transform_to_intensity, data, i0, stream)
+
+    def poisson_noise(self, data, i0_per_module, seed: int, stream: int = 0):
+        """PoissonNoiseExtension's noise on extinction data [view][module][rows][channels]
+        in place; i0_per_module: photons per pixel of each module."""
+        data = self._inplace_f32(data)
+        V, M = int(data.shape[0]), int(data.shape[1])
+        ppm = int(np.prod(tuple(data.shape[2:])))
+        i0 = np.ascontiguousarray(np.broadcast_to(np.asarray(i0_per_module, np.float32), (M,)))
+        stream = self._stream_for(stream, data)
+        self._check(self.lib.ctlcu_poisson_noise(self.h, C.c_void_p(_ptr(data)), V, M, ppm,
+                                                 C.c_void_p(i0.ctypes.data), C.c_uint64(int(seed)),
+                                                 C.c_void_p(stream or None)))
+        return data
+
     def project_volume(self, vol: VoxelVolume, pmats, channels: int, rows: int,
                        settings: Optional[Settings] = None, out=None):
         """One-shot: upload, project, release (the reference's per-call semantics)."""

@@ -223,6 +223,37 @@ CTLCU_API int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_v
 /* Number of kernels this library has launched on the context (all calls). */
 CTLCU_API int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches);
 
+/* ---- post-projection operations ---------------------------------------------------------- */
+
+/*
+ * ProjectionData::transformToExtinction / transformToIntensity with one i0 per
+ * view (img/projectiondata.cpp; img/singleviewdata.cpp:135-172), in place over
+ * n_views x values_per_view floats: p = log(i0 / p) or p = i0 exp(-p), in FP32
+ * like the reference.  i0: n_views doubles in host memory, or NULL for i0 = 1.
+ * data: device memory (asynchronous on `stream`, NULL = the context's stream)
+ * or host memory (returns when done).
+ */
+CTLCU_API int ctlcu_transform_to_extinction(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
+                                            const double* i0, void* stream);
+CTLCU_API int ctlcu_transform_to_intensity(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
+                                           const double* i0, void* stream);
+
+/*
+ * PoissonNoiseExtension (projectors/poissonnoiseextension.cpp:35-68, :156-198) on
+ * extinction data [view][module][pixel] in place: per pixel, count =
+ * i0[module] exp(-p), noisy ~ Poisson(count) for count < 1e4 and
+ * Normal(count, sqrt(count)) above, p = log(i0[module] / noisy).  A zero
+ * count sum leaves the data unchanged, as the reference skips such views.
+ * i0_per_module: n_modules photons per pixel (RadiationEncoder::photonsPerPixel),
+ * host memory.  The noise of a pixel is a fixed function of (seed, view,
+ * pixel): counter-based Philox4x32-10 streams instead of the reference's
+ * per-view mt19937_64 (same distributions, different draws).  data: device
+ * (asynchronous on `stream`) or host memory (returns when done).
+ */
+CTLCU_API int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t n_modules,
+                                  uint32_t pixels_per_module, const float* i0_per_module, uint64_t seed,
+                                  void* stream);
+
 /* ---- geometry encoding ------------------------------------------------------------------- */
 
 /* Detector of a simple CT system: CylindricalDetector(nbPixelPerModule,

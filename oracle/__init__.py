@@ -121,3 +121,43 @@ def view_setup(pmats, which="fp64"):
         _lib(os.path.join("_ref", "libctlref.so")).ctlref_view_setup(
             P.ctypes.data_as(dp), C.c_uint(V), C.c_uint(M), qr.ctypes.data_as(dp), src.ctypes.data_as(dp))
     return qr, src
+
+
+def poisson_noise(extinction, i0_per_module, seed):
+    """The device noise algorithm restated on the CPU (postops_oracle.c):
+    returns (noisy extinction, noisy counts), both [V, M, rows, channels]."""
+    x = np.array(extinction, dtype=np.float32, copy=True, order="C")
+    V, M = x.shape[0], x.shape[1]
+    ppm = int(np.prod(x.shape[2:]))
+    i0 = np.ascontiguousarray(i0_per_module, dtype=np.float32)
+    counts = np.empty_like(x)
+    fp = C.POINTER(C.c_float)
+    _lib("liboracle.so").oracle_poisson_noise(x.ctypes.data_as(fp), C.c_uint(V), C.c_uint(M), C.c_uint(ppm),
+                                              i0.ctypes.data_as(fp), C.c_uint64(seed), counts.ctypes.data_as(fp))
+    return x, counts
+
+
+def poisson_draws(lam, seed, view=0):
+    """Draws of the device sampler (one counter stream per entry) for the means `lam`."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64).ravel()
+    out = np.empty(lam.size, np.float32)
+    _lib("liboracle.so").oracle_poisson_draws(lam.ctypes.data_as(C.POINTER(C.c_double)), C.c_uint64(lam.size),
+                                              C.c_uint64(seed), C.c_uint(view),
+                                              out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def poisson_noise_reference(extinction, i0_per_module, seed):
+    """The reference's noise step with its own mt19937_64 and std:: distributions
+    (poisson_ref.cpp): noisy extinction [V, M, rows, channels]."""
+    x = np.array(extinction, dtype=np.float32, copy=True, order="C")
+    V, M = x.shape[0], x.shape[1]
+    ppm = int(np.prod(x.shape[2:]))
+    i0 = np.ascontiguousarray(i0_per_module, dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    path = os.path.join(_HERE, "libpoissonref.so")
+    if not os.path.exists(path):
+        build(with_ref=False)
+    C.CDLL(path).ref_poisson_noise(x.ctypes.data_as(fp), C.c_uint(V), C.c_uint(M), C.c_uint(ppm),
+                                   i0.ctypes.data_as(fp), C.c_uint(seed))
+    return x
