@@ -515,6 +515,75 @@ def run_postops(args):
     ctx.close()
 
 
+def run_den(args):
+    """The 360 x 512^2 projections written to a DEN file straight from device memory
+    (ctlcu_den_write: pinned double-buffered staging, copies overlapping the writes),
+    against CTL's path: every view copied to a host ProjectionData, then written."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from ctl_b200 import den as D
+    from ctl_b200.projector import Context
+    ctx = Context(0)
+    rng = np.random.default_rng(5)
+    dev = torch.from_numpy(rng.random((N_VIEWS, 1, ROWS, CHANNELS), dtype=np.float32)).cuda()
+    nbytes = dev.numel() * 4
+    tmp = tempfile.mkdtemp(prefix="den_bench_")
+    try:
+        path = os.path.join(tmp, "proj.den")
+        times = []
+        for i in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            D.save_projections(ctx, dev, path)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+        # CTL's order of work: per-view device->host copies into host memory, then the file
+        ref = []
+        host = np.empty((N_VIEWS, 1, ROWS, CHANNELS), np.float32)
+        for i in range(max(1, min(3, args.steps))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for v in range(N_VIEWS):
+                host[v] = dev[v].cpu().numpy()
+            D.write_den(os.path.join(tmp, "ref.den"), host.reshape(N_VIEWS, ROWS, CHANNELS))
+            ref.append(time.perf_counter() - t0)
+        t = statistics.mean(times)
+        # the same two paths into /dev/null: the copy pipeline without the file system
+        null = []
+        for i in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            D.save_projections(ctx, dev, "/dev/null")
+            null.append(time.perf_counter() - t0)
+        null_ref = []
+        for i in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for v in range(N_VIEWS):
+                host[v] = dev[v].cpu().numpy()
+            D.write_den("/dev/null", host.reshape(N_VIEWS, ROWS, CHANNELS))
+            null_ref.append(time.perf_counter() - t0)
+        extra = {"e2e": {"value": nbytes / t / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": int(nbytes), "path": "ctlcu_den_write from device memory"},
+                 "gpu_launches": 0,
+                 "per_view_copy_then_write_gb_s": nbytes / statistics.mean(ref) / 1e9,
+                 "to_dev_null_gb_s": nbytes / min(null) / 1e9,
+                 "per_view_copy_then_write_to_dev_null_gb_s": nbytes / min(null_ref) / 1e9,
+                 "target": f"{tmp} (page cache; no fsync)",
+                 "roofline": {"bound": "pcie/host", "achieved": nbytes / t / 1e9, "unit": "GB/s",
+                              "note": "device-to-host copies and file writes, overlapped; no kernel"}}
+        _line("GB/s writing 360 x 512^2 float32 projections to a DEN file from device memory",
+              nbytes / t / 1e9, "GB/s", t * 1e3, args,
+              {"workload": "360 x 512 x 512 float32 projections (377 MB) -> DEN file"}, **extra)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        ctx.close()
+
+
 def hbm_peak() -> float:
     """The measured HBM copy bandwidth of this pool's B200s (GB/s), else the fallback."""
     try:
@@ -624,7 +693,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5", "geometry", "postops"], default="c2",
+    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5", "geometry", "postops", "den"], default="c2",
                     help="c2 (default) is the headline; the others print extra lines")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
@@ -640,6 +709,8 @@ def main():
         return run_geometry(args)
     if args.config == "postops":
         return run_postops(args)
+    if args.config == "den":
+        return run_den(args)
     return run_ours(args)
 
 

@@ -64,6 +64,7 @@ struct ctlcu_ctx {
     cudaEvent_t order = nullptr;  // orders caller streams after volume staging on `stream`
     // autotuned sample-loop choice per (volume, channels, rows, modules)
     std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, int> tuned;
+    DenStaging den;  // pinned buffers for DEN file streaming, allocated on first use
 };
 
 namespace {
@@ -884,6 +885,7 @@ int ctlcu_destroy(ctlcu_ctx* ctx)
         cudaFree(ctx->d_counter);
         if (ctx->order)
             cudaEventDestroy(ctx->order);
+        ctx->den.release();
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -1394,6 +1396,53 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
     std::lock_guard<std::mutex> lk(ctx->mu);
     *launches = ctx->launches;
     return CTLCU_OK;
+}
+
+int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t elem_bytes, uint32_t rows,
+                    uint32_t cols, uint32_t count, void* stream)
+{
+    if (!ctx) {
+        // host data needs no context (nor a GPU)
+        if (!path || !data || is_device_ptr(data))
+            return CTLCU_ERR_INVALID_ARGUMENT;
+        std::string msg;
+        return den_write(path, data, elem_bytes, rows, cols, count, nullptr, nullptr, msg);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!path || !data)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "path or data is NULL");
+    cudaSetDevice(ctx->device);
+    std::string msg;
+    const int r = den_write(path, data, elem_bytes, rows, cols, count, stream ? (cudaStream_t)stream : ctx->stream,
+                            &ctx->den, msg);
+    return r ? fail(ctx, r, "DEN write: %s", msg.c_str()) : CTLCU_OK;
+}
+
+int ctlcu_den_header(const char* path, uint32_t dims[3], uint32_t* elem_bytes)
+{
+    if (!path || !dims || !elem_bytes)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::string msg;
+    return den_header(path, dims, elem_bytes, msg);
+}
+
+int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, uint32_t first, uint32_t n,
+                   void* stream)
+{
+    if (!ctx) {
+        if (!path || !data || is_device_ptr(data))
+            return CTLCU_ERR_INVALID_ARGUMENT;
+        std::string msg;
+        return den_read(path, data, capacity_bytes, first, n, nullptr, nullptr, msg);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!path || !data)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "path or data is NULL");
+    cudaSetDevice(ctx->device);
+    std::string msg;
+    const int r = den_read(path, data, capacity_bytes, first, n, stream ? (cudaStream_t)stream : ctx->stream,
+                           &ctx->den, msg);
+    return r ? fail(ctx, r, "DEN read: %s", msg.c_str()) : CTLCU_OK;
 }
 
 int ctlcu_transform_to_extinction(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,

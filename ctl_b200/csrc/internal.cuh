@@ -240,5 +240,24 @@ cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modul
                                  uint64_t seed, cudaStream_t s);
 cudaError_t launch_transform(float* data, uint64_t per_view, uint32_t n_views, const double* i0, bool to_extinction,
                              cudaStream_t s);
+}  // namespace ctlcu
+
+#include <string>
+
+namespace ctlcu {
+// Two pinned host buffers and their events for streaming device data to and
+// from files; a context keeps one, allocated on first use.
+struct DenStaging {
+    static constexpr size_t kBytes = 32u << 20;  // per buffer
+    void* buf[2] = { nullptr, nullptr };
+    cudaEvent_t ev[2] = { nullptr, nullptr };
+    cudaError_t ensure();
+    void release();
+};
+int den_write(const char* path, const void* data, uint32_t elem, uint32_t rows, uint32_t cols, uint32_t count,
+              cudaStream_t st, DenStaging* stage, std::string& msg);
+int den_header(const char* path, uint32_t dims[3], uint32_t* elem, std::string& msg);
+int den_read(const char* path, void* data, uint64_t capacity, uint32_t first, uint32_t n_mats, cudaStream_t st,
+             DenStaging* stage, std::string& msg);
 
 }  // namespace ctlcu

@@ -254,6 +254,34 @@ CTLCU_API int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views,
                                   uint32_t pixels_per_module, const float* i0_per_module, uint64_t seed,
                                   void* stream);
 
+/* ---- DEN files ---------------------------------------------------------------------------- */
+
+/*
+ * io::den::DFileFormat::save (io/den/dfileformat.tpp:148-187): writes `count`
+ * row-major rows x cols matrices of elem_bytes-sized elements (1, 2, 4 or 8:
+ * uchar, ushort, float, double) behind the 6-byte uint16 header.  data may be
+ * device memory: it is streamed to the file through pinned staging buffers
+ * (copies overlap the writes), ordered after earlier work on `stream` (NULL =
+ * the context's stream).  Projections [view][module][row][channel] are
+ * rows = detector rows, cols = channels, count = views x modules, as CTL's
+ * DenFileIO writes them (io/den/denfileio.h:53-68).  Returns when the file is
+ * complete; dimensions above 65535 are rejected, as in the reference.  ctx may
+ * be NULL for host data (no GPU needed).
+ */
+CTLCU_API int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t elem_bytes, uint32_t rows,
+                              uint32_t cols, uint32_t count, void* stream);
+
+/* io::den::loadHeader + getDataType (io/den/den_header.tpp:51-80, den_utils.tpp:8-24):
+ * dims = {rows, cols, count}; elem_bytes from the data size. */
+CTLCU_API int ctlcu_den_header(const char* path, uint32_t dims[3], uint32_t* elem_bytes);
+
+/* DFileFormat::load (io/den/dfileformat.tpp): matrices first .. first+n-1 (n = 0: to the
+ * end) into `data` (device memory, filled through pinned staging buffers, or host
+ * memory) of capacity_bytes.  Returns when the data is in place.  ctx may be NULL
+ * for host data. */
+CTLCU_API int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, uint32_t first,
+                             uint32_t n, void* stream);
+
 /* ---- geometry encoding ------------------------------------------------------------------- */
 
 /* Detector of a simple CT system: CylindricalDetector(nbPixelPerModule,

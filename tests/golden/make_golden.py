@@ -1,7 +1,8 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
     make -C oracle all ref          # builds oracle/_ref/libctlref.so from the reference sources
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # everything
+    python tests/golden/make_golden.py den      # den_files.json only
 
 Needs the reference sources at /root/reference (only where this script runs;
 the tests read the .npz files it writes, never the reference).
@@ -17,9 +18,12 @@ Writes
                    of the reference's own ray_caster kernels
                    (raycasterprojector_interp.cl / _no_interp.cl run through
                    oracle/ref_harness.cpp)
+  den_files.json   size, header and SHA-256 of testing/testData/tubeGeo.den and
+                   cArmGeo.den (the DEN writer must reproduce them byte for byte)
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import sys
@@ -91,7 +95,23 @@ def main():
         print(f"{name}: {ref.shape} max {ref.max():.4f}")
     arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     np.savez_compressed(os.path.join(HERE, "projections.npz"), **arrays)
+    den_files()
+
+
+def den_files():
+    """den_files.json: size, header and SHA-256 of the reference's golden DEN files,
+    so the DEN writer can be checked byte for byte without the files."""
+    out = {}
+    for name in ("tubeGeo.den", "cArmGeo.den"):
+        raw = open(os.path.join(TESTDATA, name), "rb").read()
+        out[name] = {"bytes": len(raw), "header": [int(v) for v in np.frombuffer(raw[:6], "<u2")],
+                     "sha256": hashlib.sha256(raw).hexdigest()}
+    with open(os.path.join(HERE, "den_files.json"), "w") as f:
+        json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["den"]:
+        den_files()
+    else:
+        main()
