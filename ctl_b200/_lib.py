@@ -118,6 +118,10 @@ SIGNATURES = [
                                                C.c_void_p]),
     ("ctlcu_poisson_noise", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
                                       C.c_uint64, C.c_void_p]),
+    ("ctlcu_encode_geometry_shifted", C.c_int, [C.c_void_p, C.POINTER(DetectorDesc), C.POINTER(TrajectoryDesc),
+                                                C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("ctlcu_average_samples", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_int,
+                                        C.c_void_p]),
     ("ctlcu_den_write", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                   C.c_uint32, C.c_void_p]),
     ("ctlcu_den_header", C.c_int, [C.c_char_p, C.POINTER(C.c_uint32 * 3), C.POINTER(C.c_uint32)]),

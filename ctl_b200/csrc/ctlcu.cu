@@ -1398,6 +1398,23 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
     return CTLCU_OK;
 }
 
+int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, uint64_t values_per_sample,
+                          float* out, int low_extinction, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!in || !out || n_samples == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "in/out is NULL or no samples");
+    cudaSetDevice(ctx->device);
+    if (!is_device_ptr(in) || !is_device_ptr(out))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "in and out must be device memory");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    CU_TRY(ctx, launch_average_samples(in, n_samples, values_per_sample, out, low_extinction != 0, st));
+    ++ctx->launches;
+    return CTLCU_OK;
+}
+
 int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t elem_bytes, uint32_t rows,
                     uint32_t cols, uint32_t count, void* stream)
 {
@@ -1494,9 +1511,22 @@ int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t 
 int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
                           const ctlcu_trajectory_desc* trajectory, uint32_t n_views, double* pmats, void* stream)
 {
+    return ctlcu_encode_geometry_shifted(ctx, detector, trajectory, n_views, nullptr, 0, pmats, stream);
+}
+
+int ctlcu_encode_geometry_shifted(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
+                                  const ctlcu_trajectory_desc* trajectory, uint32_t n_views,
+                                  const double* source_shifts_mm, uint32_t n_shifts, double* pmats, void* stream)
+{
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    if (source_shifts_mm && n_shifts == 0)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "n_shifts is 0");
+    for (uint32_t k = 0; source_shifts_mm && k < 3 * n_shifts; ++k)
+        if (!std::isfinite(source_shifts_mm[k]))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "source shifts must be finite");
+    const uint32_t shifts = source_shifts_mm ? n_shifts : 1u;
     if (!detector || !trajectory || !pmats)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "detector, trajectory or pmats is NULL");
     const ctlcu_detector_desc& d = *detector;
@@ -1523,18 +1553,28 @@ int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "a C-arm gantry needs a positive C-arm span");
     if (t.kind == CTLCU_TRAJ_CIRCLE_PLUS_LINE && !(t.line_fraction >= 0.0 && t.line_fraction <= 1.0))
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "line_fraction must lie in [0, 1]");
-    const uint64_t n = (uint64_t)n_views * d.n_modules;
+    const uint64_t n = (uint64_t)n_views * d.n_modules * shifts;
     if (n > 0x7fffffffull)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many matrices");
     cudaSetDevice(ctx->device);
     const bool dev = is_device_ptr(pmats);
     cudaStream_t st = dev && stream ? (cudaStream_t)stream : ctx->stream;
     double* out = pmats;
+    double* d_shifts = nullptr;
     if (!dev)
         CU_TRY(ctx, cudaMallocAsync((void**)&out, n * 12 * sizeof(double), st));
-    cudaError_t e = launch_encode_geometry(d, t, n_views, out, st);
+    cudaError_t e = cudaSuccess;
+    if (source_shifts_mm) {
+        e = cudaMallocAsync((void**)&d_shifts, sizeof(double) * 3 * shifts, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_shifts, source_shifts_mm, sizeof(double) * 3 * shifts, cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess)
+        e = launch_encode_geometry(d, t, n_views, d_shifts, shifts, out, st);
     if (e == cudaSuccess && !dev)
         e = cudaMemcpyAsync(pmats, out, n * 12 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (d_shifts)
+        cudaFreeAsync(d_shifts, st);
     if (!dev)
         cudaFreeAsync(out, st);
     if (e != cudaSuccess)

@@ -78,10 +78,13 @@ struct GeoArgs {
     double short_span;  // angle span of a short scan (after the fan-angle default)
     uint32_t n_line;    // circle-plus-line: views on the line
     float axial_inc;    // axial scan: the reference's float increment
+    const double* shifts;  // n_shifts source displacements (x, y, z) in the source frame, or null
+    uint32_t n_shifts;     // >= 1; output [shift][view][module]
 };
 
 struct Gantry {
     V3 src;      // source position (world)
+    M3 src_rot;  // source frame -> world (active): a source displacement moves along it
     V3 det;      // detector centre (world)
     M3 det_rot;  // world -> detector CT coordinates (passive)
 };
@@ -94,6 +97,7 @@ __device__ inline Gantry tubular(double angle, double pitch, const ctlcu_traject
     Gantry g;
     g.src = mul(G, V3{ t.sid_mm, 0.0, -pitch });
     g.det = mul(G, V3{ -(t.sdd_mm - t.sid_mm), 0.0, -pitch });
+    g.src_rot = S;
     g.det_rot = tr(S);
     return g;
 }
@@ -105,6 +109,7 @@ __device__ inline Gantry carm(const V3& pos, const M3& R, double span)
     g.src = pos;
     const V3 off = mul(R, V3{ 0.0, 0.0, -span });
     g.det = V3{ pos.x - off.x, pos.y - off.y, pos.z - off.z };
+    g.src_rot = R;
     g.det_rot = tr(R);
     return g;
 }
@@ -155,11 +160,21 @@ __device__ inline Gantry gantry_state(const GeoArgs& a, uint32_t v)
 __global__ void encode_kernel(const GeoArgs a, double* __restrict__ pmats)
 {
     const uint32_t M = a.det.n_modules;
+    const uint64_t per_shift = (uint64_t)a.n_views * M;
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= (uint64_t)a.n_views * M)
+    if (i >= per_shift * a.n_shifts)
         return;
-    const uint32_t v = (uint32_t)(i / M), m = (uint32_t)(i - (uint64_t)v * M);
-    const Gantry g = gantry_state(a, v);
+    const uint32_t sh = (uint32_t)(i / per_shift);
+    const uint64_t j = i - (uint64_t)sh * per_shift;
+    const uint32_t v = (uint32_t)(j / M), m = (uint32_t)(j - (uint64_t)v * M);
+    Gantry g = gantry_state(a, v);
+    if (a.shifts) {
+        // a source displacement (position only) added to the prepared gantry: the
+        // source moves by sourceRotation * shift (abstractgantry.h:159-164,
+        // preparesteps.cpp:202-210)
+        const V3 d = mul(g.src_rot, V3{ a.shifts[3 * sh], a.shifts[3 * sh + 1], a.shifts[3 * sh + 2] });
+        g.src = V3{ g.src.x + d.x, g.src.y + d.y, g.src.z + d.z };
+    }
 
     // module location (cylindricaldetector.cpp:104-140; flat panel: origin, identity)
     V3 p{ 0.0, 0.0, 0.0 };
@@ -205,9 +220,12 @@ __global__ void encode_kernel(const GeoArgs a, double* __restrict__ pmats)
 // Host-side constants of the system (radius, short-scan span, line views,
 // axial float increment), then one launch over views x modules.
 cudaError_t launch_encode_geometry(const ctlcu_detector_desc& det, const ctlcu_trajectory_desc& traj,
-                                   uint32_t n_views, double* pmats, cudaStream_t s)
+                                   uint32_t n_views, const double* d_shifts, uint32_t n_shifts, double* pmats,
+                                   cudaStream_t s)
 {
     GeoArgs a = {};
+    a.shifts = d_shifts;
+    a.n_shifts = d_shifts ? n_shifts : 1u;
     a.det = det;
     a.traj = traj;
     a.n_views = n_views;
@@ -232,7 +250,7 @@ cudaError_t launch_encode_geometry(const ctlcu_detector_desc& det, const ctlcu_t
     }
     a.n_line = (uint32_t)floor(n_views * traj.line_fraction);
     a.axial_inc = n_views > 0 ? (float)(2.0 * kPi / double(n_views)) : 0.0f;
-    const uint64_t total = (uint64_t)n_views * det.n_modules;
+    const uint64_t total = (uint64_t)n_views * det.n_modules * a.n_shifts;
     if (total == 0)
         return cudaSuccess;
     const unsigned threads = 128;

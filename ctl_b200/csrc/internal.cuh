@@ -235,7 +235,10 @@ cudaError_t launch_build_pairs(const void* padded, const int n[3], int dtype, co
 cudaError_t launch_unpad_upsample(const void* padded, const int n[3], int dtype, int f, void* dst,
                                   cudaStream_t s);
 cudaError_t launch_encode_geometry(const ctlcu_detector_desc& det, const ctlcu_trajectory_desc& traj,
-                                   uint32_t n_views, double* pmats, cudaStream_t s);
+                                   uint32_t n_views, const double* d_shifts, uint32_t n_shifts, double* pmats,
+                                   cudaStream_t s);
+cudaError_t launch_average_samples(const float* in, uint32_t n_samples, uint64_t n, float* out, bool low_extinction,
+                                   cudaStream_t s);
 cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modules, uint32_t ppm, const float* i0,
                                  uint64_t seed, cudaStream_t s);
 cudaError_t launch_transform(float* data, uint64_t per_view, uint32_t n_views, const double* i0, bool to_extinction,

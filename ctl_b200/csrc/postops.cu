@@ -137,6 +137,24 @@ __global__ void intensity_kernel(float* __restrict__ data, uint64_t per_view, ui
     }
 }
 
+// ArealFocalSpotExtension::extendedProject (projectors/arealfocalspotextension.cpp:82-160):
+// the projections of the focal-spot samples averaged in intensity domain
+// (exp(-p) summed in sample order, divided by the count, log(1 / x)), or in
+// extinction domain with the low-extinction approximation.  in: [sample][n].
+__global__ void average_kernel(const float* __restrict__ in, uint32_t n_samples, uint64_t n, float* __restrict__ out,
+                               int low_extinction)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (uint32_t s = 0; s < n_samples; ++s) {
+            const float p = in[(uint64_t)s * n + i];
+            acc += low_extinction ? p : expf(-p);
+        }
+        acc /= (float)n_samples;
+        out[i] = low_extinction ? acc : logf(1.0f / acc);
+    }
+}
+
 unsigned grid_for_elements(uint64_t n)
 {
     uint64_t b = (n + 255) / 256;
@@ -154,6 +172,15 @@ cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modul
         return cudaSuccess;
     poisson_kernel<<<grid_for_elements(total), 256, 0, s>>>(data, n_views, n_modules, ppm, i0, (uint32_t)seed,
                                                              (uint32_t)(seed >> 32));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_average_samples(const float* in, uint32_t n_samples, uint64_t n, float* out, bool low_extinction,
+                                   cudaStream_t s)
+{
+    if (n == 0 || n_samples == 0)
+        return cudaSuccess;
+    average_kernel<<<grid_for_elements(n), 256, 0, s>>>(in, n_samples, n, out, low_extinction ? 1 : 0);
     return cudaGetLastError();
 }
 

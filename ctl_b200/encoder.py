@@ -172,13 +172,17 @@ class AcquisitionSetup:
 
 class GeometryEncoder:
     @staticmethod
-    def encode_full_geometry(setup: AcquisitionSetup, ctx, out=None, stream: int = 0):
+    def encode_full_geometry(setup: AcquisitionSetup, ctx, out=None, stream: int = 0, source_shifts=None):
         """All views' projection matrices, (views, modules, 3, 4) float64.
         `out` may be a device tensor (filled asynchronously on torch's current
-        stream, or `stream`) or a numpy array; by default a new numpy array."""
+        stream, or `stream`) or a numpy array; by default a new numpy array.
+        source_shifts: (n, 3) source displacements in mm in the source's frame;
+        then the result is (n * views, modules, 3, 4), shift-major."""
         from .projector import _is_cuda, _ptr, torch_stream_handle
         dd, t = setup.descriptors()
-        shape = (setup.nb_views, setup.nb_modules(), 3, 4)
+        shifts = None if source_shifts is None else np.ascontiguousarray(source_shifts, np.float64).reshape(-1, 3)
+        n_sh = 1 if shifts is None else shifts.shape[0]
+        shape = (n_sh * setup.nb_views, setup.nb_modules(), 3, 4)
         if out is None:
             out = np.empty(shape, np.float64)
         if tuple(out.shape) != shape:
@@ -186,6 +190,11 @@ class GeometryEncoder:
         if not stream and _is_cuda(out):
             import torch
             stream = torch_stream_handle(torch.cuda.current_stream(out.device))
-        ctx._check(ctx.lib.ctlcu_encode_geometry(ctx.h, C.byref(dd), C.byref(t), setup.nb_views,
-                                                 C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
+        if shifts is None:
+            ctx._check(ctx.lib.ctlcu_encode_geometry(ctx.h, C.byref(dd), C.byref(t), setup.nb_views,
+                                                     C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
+        else:
+            ctx._check(ctx.lib.ctlcu_encode_geometry_shifted(
+                ctx.h, C.byref(dd), C.byref(t), setup.nb_views, C.c_void_p(shifts.ctypes.data), n_sh,
+                C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
         return out

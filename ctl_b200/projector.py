@@ -388,6 +388,18 @@ class Context:
         """ProjectionData::transformToIntensity: p = i0 exp(-p) in place."""
         return self._transform(self.lib.ctlcu_transform_to_intensity, data, i0, stream)
 
+    def average_samples(self, data, n_samples: int, out, low_extinction: bool = False, stream: int = 0):
+        """ArealFocalSpotExtension's averaging of n_samples projection sets
+        (data: device tensor [sample * views, ...]) into `out` (device, [views, ...])."""
+        per = int(out.numel())
+        if int(data.numel()) != per * n_samples:
+            raise ValueError("data must hold n_samples times the values of out")
+        stream = self._stream_for(stream, data, out)
+        self._check(self.lib.ctlcu_average_samples(self.h, C.c_void_p(_ptr(data)), int(n_samples), per,
+                                                   C.c_void_p(_ptr(out)), 1 if low_extinction else 0,
+                                                   C.c_void_p(stream or None)))
+        return out
+
     def poisson_noise(self, data, i0_per_module, seed: int, stream: int = 0):
         """PoissonNoiseExtension's noise on extinction data [view][module][rows][channels]
         in place; i0_per_module: photons per pixel of each module."""

@@ -335,6 +335,24 @@ CTLCU_API int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* d
                                     const ctlcu_trajectory_desc* trajectory, uint32_t n_views, double* pmats,
                                     void* stream);
 
+/* The same for n_shifts source displacements at once: each shift (x, y, z in mm,
+ * in the source's own frame, host memory) is added to the prepared gantry's source
+ * displacement as a GantryDisplacementParam increment does
+ * (acquisition/preparesteps.cpp:202-210, components/abstractgantry.h:159-164);
+ * ArealFocalSpotExtension uses this for its focal-spot samples
+ * (projectors/arealfocalspotextension.cpp:108-127).  pmats: [shift][view][module]. */
+CTLCU_API int ctlcu_encode_geometry_shifted(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
+                                            const ctlcu_trajectory_desc* trajectory, uint32_t n_views,
+                                            const double* source_shifts_mm, uint32_t n_shifts, double* pmats,
+                                            void* stream);
+
+/* ArealFocalSpotExtension's averaging (projectors/arealfocalspotextension.cpp:127-160):
+ * out[i] = -log(mean_s exp(-in[s][i])) over n_samples projections [sample][values]
+ * (intensity domain), or mean_s in[s][i] with low_extinction != 0.  Device memory,
+ * asynchronous on `stream` (NULL = the context's stream). */
+CTLCU_API int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, uint64_t values_per_sample,
+                                    float* out, int low_extinction, void* stream);
+
 /*
  * No counterpart in the reference.  ctlcu_project for callers that cannot
  * allocate device memory while they run: a real-time loop that reserved all

@@ -112,20 +112,20 @@ class Trajectory:
 
 
 def _tubular(rotation_angle, pitch, tilt, sdd, sid):
-    """Source position/rotation and detector position/passive rotation of a
-    TubularGantry (tubulargantry.cpp:53-90)."""
+    """Source position, detector position, detector passive rotation and source
+    rotation of a TubularGantry (tubulargantry.cpp:53-90)."""
     G = rotation(tilt, "x") @ rotation(rotation_angle, "z")
     src = G @ np.array([sid, 0.0, -pitch])
     src_rot = G @ rotation(PI_2, "z") @ rotation(-PI_2, "x")
     det = G @ np.array([-(sdd - sid), 0.0, -pitch])
     det_rot = (G @ rotation(PI_2, "z") @ rotation(-PI_2, "x")).T
-    return src, det, det_rot
+    return src, det, det_rot, src_rot
 
 
 def _carm(position, rot, span):
     """CarmGantry with location (position, rot) (carmgantry.cpp:34-71)."""
     det = position - rot @ np.array([0.0, 0.0, -span])
-    return position, det, rot.T
+    return position, det, rot.T, rot
 
 
 def _fixed(start_angle):
@@ -191,13 +191,18 @@ def intrinsic(dev, det: Detector) -> np.ndarray:
     return np.array([[fx, det.skew, px], [0.0, fy, py], [0.0, 0.0, 1.0]])
 
 
-def encode_full_geometry(det: Detector, traj: Trajectory, n_views: int) -> np.ndarray:
+def encode_full_geometry(det: Detector, traj: Trajectory, n_views: int, source_shift=None) -> np.ndarray:
     """(n_views, modules, 3, 4) normalised projection matrices
-    (geometryencoder.cpp:67-117, projectionmatrix.cpp:44-48, :125-131)."""
+    (geometryencoder.cpp:67-117, projectionmatrix.cpp:44-48, :125-131).
+    source_shift: a source displacement (x, y, z) in the source frame, added to
+    the prepared gantry as a GantryDisplacementParam increment does
+    (preparesteps.cpp:202-210; abstractgantry.h:159-164)."""
     locs = det.module_locations()
     out = np.zeros((n_views, len(locs), 3, 4))
     for v in range(n_views):
-        src, det_pos, det_rot = gantry_state(traj, v, n_views, det)
+        src, det_pos, det_rot, src_rot = gantry_state(traj, v, n_views, det)
+        if source_shift is not None:
+            src = src + src_rot @ np.asarray(source_shift, np.float64)
         for m, (p, R) in enumerate(locs):
             mod_pos = det_pos + det_rot.T @ p
             tot = R @ det_rot
@@ -236,3 +241,11 @@ def golden_carm_setup():
     traj = Trajectory("wobble", carm_span=1200.0, source_to_iso=750.0, angle_span=math.radians(200.0),
                       start_angle=0.0, wobble_angle=math.radians(20.0), wobble_freq=5.0)
     return det, traj, 30
+
+
+def focal_spot_grid(nx: int, ny: int):
+    """ArealFocalSpotExtension::discretizationGrid (arealfocalspotextension.cpp):
+    nx x ny points in [-1/2, 1/2]^2, x outer, y inner (one point: the centre)."""
+    xs = [-0.5 + i / (nx - 1) for i in range(nx)] if nx > 1 else [0.0]
+    ys = [-0.5 + j / (ny - 1) for j in range(ny)] if ny > 1 else [0.0]
+    return [(x, y) for x in xs for y in ys]

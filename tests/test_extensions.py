@@ -1,0 +1,124 @@
+"""Extension chains as batched device work: ArealFocalSpotExtension (and Poisson
+noise on its result), against the oracle and with the reference's own
+statistical test strategy (testing/src/projectortest.cpp:149-234).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import geometry_oracle as GO
+from tests._common import rel_err
+
+TOL = 1e-4
+
+
+def test_discretization_grid_matches_the_oracle_restatement():
+    from ctl_b200.extensions import discretization_grid
+    for nx, ny in ((1, 1), (2, 2), (3, 1), (1, 4), (3, 5)):
+        assert discretization_grid(nx, ny) == GO.focal_spot_grid(nx, ny)
+    assert discretization_grid(2, 2) == [(-0.5, -0.5), (-0.5, 0.5), (0.5, -0.5), (0.5, 0.5)]
+
+
+def test_oracle_source_shift_moves_the_decomposed_source():
+    """The source that the reference's decomposition recovers from a shifted
+    matrix is the gantry's source moved by sourceRotation * shift."""
+    det = GO.Detector(64, 48, 2.0, 2.0, flat_panel=True)
+    traj = GO.Trajectory("short_scan", carm_span=1200.0, source_to_iso=750.0, angle_span=math.radians(90.0))
+    shift = np.array([2.5, -1.5, 0.0])
+    P = GO.encode_full_geometry(det, traj, 5, source_shift=shift)
+    _, src = oracle.view_setup(P)
+    for v in range(5):
+        s0, _, _, R = GO.gantry_state(traj, v, 5, det)
+        np.testing.assert_allclose(src[v], s0 + R @ shift, atol=1e-9)
+
+
+# ---- device ----------------------------------------------------------------------------------
+
+def _system():
+    """A 64 x 48 flat panel of 2 mm pixels on a C-arm (SID 750, span 1200), as in the
+    reference's Poisson/focal-spot test, over a short arc."""
+    from ctl_b200 import encoder as E
+    det = GO.Detector(64, 48, 2.0, 2.0, flat_panel=True)
+    traj = GO.Trajectory("short_scan", carm_span=1200.0, source_to_iso=750.0, angle_span=math.radians(60.0),
+                         start_angle=math.radians(10.0))
+    setup = E.AcquisitionSetup(E.FlatPanelDetector((64, 48), (2.0, 2.0)), E.CarmGantry(1200.0), 4)
+    setup.apply_preparation_protocol(E.ShortScanTrajectory(750.0, math.radians(10.0), math.radians(60.0)))
+    return det, traj, setup
+
+
+def _volume():
+    from ctl_b200 import phantom as Ph
+    return Ph.ellipsoid_phantom((48, 48, 40), (2.0, 2.0, 2.0), 8, seed=21)
+
+
+def _oracle_focal_spot(vol, det, traj, n_views, spot, grid, low):
+    subs = []
+    for x, y in GO.focal_spot_grid(*grid):
+        P = GO.encode_full_geometry(det, traj, n_views, source_shift=(x * spot[0], y * spot[1], 0.0))
+        p, _ = oracle.project_fp64(vol, (2.0, 2.0, 2.0), P, det.channels, det.rows)
+        subs.append(p.astype(np.float64))
+    subs = np.stack(subs)
+    return subs.mean(0) if low else -np.log(np.exp(-subs).mean(0))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from ctl_b200.projector import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.gpu
+def test_shifted_device_encoder_matches_the_oracle(ctx):
+    from ctl_b200 import encoder as E
+    det, traj, setup = _system()
+    shifts = np.array([[-2.5, -2.5, 0], [-2.5, 2.5, 0], [2.5, -2.5, 0], [2.5, 2.5, 0.0]])
+    got = E.GeometryEncoder.encode_full_geometry(setup, ctx, source_shifts=shifts)
+    assert got.shape == (16, 1, 3, 4)
+    for k, s in enumerate(shifts):
+        want = GO.encode_full_geometry(det, traj, 4, source_shift=s)
+        assert GO.pmat_difference(got[4 * k: 4 * k + 4], want) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grid,low", [((2, 2), False), ((3, 2), False), ((2, 2), True), ((1, 1), False)])
+def test_focal_spot_extension_matches_the_oracle(ctx, grid, low):
+    from ctl_b200.extensions import ArealFocalSpotExtension
+    from ctl_b200.projector import VoxelVolume
+    det, traj, setup = _system()
+    vol = _volume()
+    ext = ArealFocalSpotExtension(ctx, discretization=grid, low_extinction_approximation=low)
+    ext.configure(setup, (5.0, 5.0))
+    got = ext.project(VoxelVolume(vol, (2.0, 2.0, 2.0))).cpu().numpy()
+    want = _oracle_focal_spot(vol, det, traj, 4, (5.0, 5.0), grid, low)
+    assert rel_err(got, want).max() <= TOL
+    ext.release()
+
+
+@pytest.mark.gpu
+def test_focal_spot_and_noise_follow_the_reference_test_strategy(ctx):
+    """projectortest.cpp:149-234: the same pose repeated, Poisson noise on the
+    focal-spot projections; the repetition mean of the counts matches the clean
+    counts to 1% and the mean equals the variance (Poisson)."""
+    from ctl_b200 import encoder as E
+    from ctl_b200.extensions import ArealFocalSpotExtension, PoissonNoiseExtension
+    from ctl_b200.projector import VoxelVolume
+    reps, i0 = 400, 5000.0
+    setup = E.AcquisitionSetup(E.FlatPanelDetector((50, 50), (2.0, 2.0)), E.CarmGantry(1200.0), reps)
+    setup.apply_preparation_protocol(E.ShortScanTrajectory(750.0, math.radians(30.0), 0.0))  # one pose, repeated
+    vol = VoxelVolume(_volume(), (2.0, 2.0, 2.0))
+    clean_ext = ArealFocalSpotExtension(ctx, discretization=(2, 2))
+    clean_ext.configure(setup, (5.0, 5.0))
+    clean = clean_ext.project(vol).cpu().numpy()[0, 0].astype(np.float64)
+    noisy_ext = PoissonNoiseExtension(clean_ext, i0, fixed_seed=11)
+    noisy = noisy_ext.project(vol).cpu().numpy()[:, 0].astype(np.float64)
+    counts = i0 * np.exp(-noisy)
+    clean_counts = i0 * np.exp(-clean)
+    mean, var = counts.mean(0), counts.var(0, ddof=1)
+    assert abs(mean.mean() / clean_counts.mean() - 1.0) < 0.01
+    diff = (mean - var) / mean
+    assert abs(diff.mean()) < 0.05 and diff.std() < 0.25
+    clean_ext.release()
