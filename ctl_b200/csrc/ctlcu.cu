@@ -65,6 +65,7 @@ struct ctlcu_ctx {
     // autotuned sample-loop choice per (volume, channels, rows, modules)
     std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, int> tuned;
     DenStaging den;  // pinned buffers for DEN file streaming, allocated on first use
+    cudaStream_t copy_stream = nullptr;  // device-to-host copies that overlap projection
 };
 
 namespace {
@@ -570,11 +571,43 @@ int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const d
     }
     if (!out_dev)
         CU_TRY(ctx, cudaMallocAsync((void**)&d_out, out_bytes, st));
-    int r = project_device(ctx, v, s, d_pm, V, M, C, R, d_out, st);
-    if (r == CTLCU_OK && !out_dev) {
-        cudaError_t e = cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess)
-            r = fail(ctx, CTLCU_ERR_CUDA, "copy of projections to the host failed: %s", cudaGetErrorString(e));
+    int r = CTLCU_OK;
+    if (out_dev) {
+        r = project_device(ctx, v, s, d_pm, V, M, C, R, d_out, st);
+    } else {
+        // Host output: the views go in chunks, and each chunk's copy to the host
+        // runs on the copy stream while the next chunk is projected.
+        if (!ctx->copy_stream)
+            CU_TRY(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        const uint32_t chunks = V >= 64 ? 8u : (V >= 8 ? 2u : 1u);
+        const uint32_t per = (V + chunks - 1) / chunks;
+        const size_t view_values = (size_t)M * R * C;
+        for (uint32_t first = 0; r == CTLCU_OK && first < V; first += per) {
+            const uint32_t n = std::min(per, V - first);
+            r = project_device(ctx, v, s, d_pm + (size_t)first * M * 12, n, M, C, R, d_out + first * view_values, st);
+            cudaEvent_t done = nullptr;
+            cudaError_t e = r ? cudaSuccess : cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+            if (!r && e == cudaSuccess)
+                e = cudaEventRecord(done, st);
+            if (!r && e == cudaSuccess)
+                e = cudaStreamWaitEvent(ctx->copy_stream, done, 0);
+            if (!r && e == cudaSuccess)
+                e = cudaMemcpyAsync(out + first * view_values, d_out + first * view_values,
+                                    sizeof(float) * n * view_values, cudaMemcpyDeviceToHost, ctx->copy_stream);
+            if (done)
+                cudaEventDestroy(done);
+            if (!r && e != cudaSuccess)
+                r = fail(ctx, CTLCU_ERR_CUDA, "copy of projections to the host failed: %s", cudaGetErrorString(e));
+        }
+        // the device buffer is freed on `st`: order that after the last copy
+        cudaEvent_t copied = nullptr;
+        if (cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(copied, ctx->copy_stream);
+            cudaStreamWaitEvent(st, copied, 0);
+            cudaEventDestroy(copied);
+        } else {
+            cudaStreamSynchronize(ctx->copy_stream);
+        }
     }
     if (pm_tmp)
         cudaFreeAsync(pm_tmp, st);
@@ -886,6 +919,10 @@ int ctlcu_destroy(ctlcu_ctx* ctx)
         if (ctx->order)
             cudaEventDestroy(ctx->order);
         ctx->den.release();
+        if (ctx->copy_stream) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            cudaStreamDestroy(ctx->copy_stream);
+        }
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
