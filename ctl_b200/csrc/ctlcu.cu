@@ -1452,6 +1452,32 @@ int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, u
     return CTLCU_OK;
 }
 
+int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* offset_proj, const double* times,
+                         uint32_t n_views, uint64_t values_per_view, float* out, void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!slope_proj || !offset_proj || !times || !out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n_views == 0 || values_per_view == 0)
+        return CTLCU_OK;
+    cudaSetDevice(ctx->device);
+    if (!is_device_ptr(slope_proj) || !is_device_ptr(offset_proj) || !is_device_ptr(out))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "projections must be device memory");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    double* d_t = nullptr;
+    CU_TRY(ctx, cudaMallocAsync((void**)&d_t, sizeof(double) * n_views, st));
+    cudaError_t e = cudaMemcpyAsync(d_t, times, sizeof(double) * n_views, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = launch_combine_linear(slope_proj, offset_proj, d_t, values_per_view, n_views, out, st);
+    cudaFreeAsync(d_t, st);
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "combine: %s", cudaGetErrorString(e));
+    ++ctx->launches;
+    return CTLCU_OK;
+}
+
 int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t elem_bytes, uint32_t rows,
                     uint32_t cols, uint32_t count, void* stream)
 {

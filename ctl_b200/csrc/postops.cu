@@ -155,6 +155,23 @@ __global__ void average_kernel(const float* __restrict__ in, uint32_t n_samples,
     }
 }
 
+// DynamicProjectorExtension::project over a LinearDynamicVolume
+// (projectors/dynamicprojectorextension.cpp:37-60, img/lineardynamicvolume.cpp:194-198):
+// the reference sets each view's voxels to slope * float(t_view) + offset and
+// projects that view.  The projection is linear in the voxel values, so
+// out[view] = float(t_view) * P(slope)[view] + P(offset)[view].
+__global__ void combine_kernel(const float* __restrict__ slope, const float* __restrict__ offset,
+                               const double* __restrict__ times, uint64_t per_view, uint32_t n_views,
+                               float* __restrict__ out)
+{
+    const uint64_t total = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float t = (float)times[i / per_view];
+        out[i] = fmaf(t, slope[i], offset[i]);
+    }
+}
+
 unsigned grid_for_elements(uint64_t n)
 {
     uint64_t b = (n + 255) / 256;
@@ -172,6 +189,16 @@ cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modul
         return cudaSuccess;
     poisson_kernel<<<grid_for_elements(total), 256, 0, s>>>(data, n_views, n_modules, ppm, i0, (uint32_t)seed,
                                                              (uint32_t)(seed >> 32));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_linear(const float* slope, const float* offset, const double* d_times, uint64_t per_view,
+                                  uint32_t n_views, float* out, cudaStream_t s)
+{
+    const uint64_t total = per_view * n_views;
+    if (total == 0)
+        return cudaSuccess;
+    combine_kernel<<<grid_for_elements(total), 256, 0, s>>>(slope, offset, d_times, per_view, n_views, out);
     return cudaGetLastError();
 }
 

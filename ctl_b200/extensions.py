@@ -119,6 +119,71 @@ class ArealFocalSpotExtension:
         self._resident.release()
 
 
+class LinearDynamicVolume:
+    """LinearDynamicVolume(slope, offset) (img/lineardynamicvolume.h): voxels are
+    slope * t + offset at time t (seconds); slope and offset are (Z, Y, X) float32
+    arrays (or tensors) of one shape and voxel size."""
+
+    def __init__(self, slope, offset, voxel_size: Sequence[float], volume_offset=(0.0, 0.0, 0.0)):
+        if tuple(slope.shape) != tuple(offset.shape):
+            raise ValueError("LinearDynamicVolume: offset and slope volumes have different sizes")
+        self.slope = VoxelVolume(slope, voxel_size, volume_offset)
+        self.offset = VoxelVolume(offset, voxel_size, volume_offset)
+
+    def at(self, t: float) -> VoxelVolume:
+        """The volume at time t, computed as the reference does (slope * float(t) + offset, FP32)."""
+        s, o = np.asarray(self.slope.data, np.float32), np.asarray(self.offset.data, np.float32)
+        return VoxelVolume((s * np.float32(t) + o).astype(np.float32), self.slope.voxel_size, self.slope.offset)
+
+
+class DynamicProjectorExtension:
+    """DynamicProjectorExtension (projectors/dynamicprojectorextension.cpp:37-60) around the
+    B200 projector.  The reference re-projects every view with the volume set to that
+    view's time.  For a LinearDynamicVolume the projection is linear in the voxels, so
+    all views come from two batched projections (slope and offset volumes) and one
+    combine launch; any other volume is projected as it is."""
+
+    def __init__(self, ctx: Context, settings: Optional[Settings] = None):
+        self.ctx = ctx
+        self.settings = settings or Settings()
+        self._pm = None
+        self._dims = None
+        self._times = None
+
+    def configure(self, pmats, channels: int, rows: int, time_stamps: Sequence[float]) -> None:
+        """pmats (views, modules, 3, 4) (host or device); time_stamps: one per view in
+        seconds (AcquisitionSetup::View::timeStamp)."""
+        if len(time_stamps) != int(pmats.shape[0]):
+            raise ValueError("one time stamp per view")
+        self._pm = pmats
+        self._dims = (int(channels), int(rows))
+        self._times = np.asarray(time_stamps, np.float64)
+
+    def project(self, volume):
+        import torch
+        if self._pm is None:
+            raise RuntimeError("DynamicProjectorExtension::project: configure() has not been called")
+        C_, R = self._dims
+        P = self._pm if hasattr(self._pm, "is_cuda") else torch.from_numpy(np.ascontiguousarray(self._pm)).cuda()
+        if not isinstance(volume, LinearDynamicVolume):
+            vol = self.ctx.volume(volume, self.settings.storage)
+            try:
+                return self.ctx.project(vol, P, C_, R, self.settings)
+            finally:
+                torch.cuda.synchronize()
+                vol.release()
+        vs = self.ctx.volume(volume.slope, self.settings.storage)
+        vo = self.ctx.volume(volume.offset, self.settings.storage)
+        try:
+            ps = self.ctx.project(vs, P, C_, R, self.settings)
+            po = self.ctx.project(vo, P, C_, R, self.settings)
+            return self.ctx.combine_linear(ps, po, self._times, torch.empty_like(ps))
+        finally:
+            torch.cuda.synchronize()
+            vs.release()
+            vo.release()
+
+
 class PoissonNoiseExtension:
     """PoissonNoiseExtension around a B200 projector or extension (anything with
     project(volume) returning device extinctions [views, modules, rows, channels]).

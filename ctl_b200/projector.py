@@ -400,6 +400,18 @@ class Context:
                                                    C.c_void_p(stream or None)))
         return out
 
+    def combine_linear(self, slope_proj, offset_proj, times, out, stream: int = 0):
+        """out[v] = float(times[v]) * slope_proj[v] + offset_proj[v] (device tensors
+        [views, ...]): projections of a linear dynamic volume, by linearity."""
+        V = int(out.shape[0])
+        per_view = int(out.numel()) // V
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(times, np.float64), (V,)))
+        stream = self._stream_for(stream, out)
+        self._check(self.lib.ctlcu_combine_linear(self.h, C.c_void_p(_ptr(slope_proj)), C.c_void_p(_ptr(offset_proj)),
+                                                  C.c_void_p(t.ctypes.data), V, per_view, C.c_void_p(_ptr(out)),
+                                                  C.c_void_p(stream or None)))
+        return out
+
     def poisson_noise(self, data, i0_per_module, seed: int, stream: int = 0):
         """PoissonNoiseExtension's noise on extinction data [view][module][rows][channels]
         in place; i0_per_module: photons per pixel of each module."""

@@ -353,6 +353,16 @@ CTLCU_API int ctlcu_encode_geometry_shifted(ctlcu_ctx* ctx, const ctlcu_detector
 CTLCU_API int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, uint64_t values_per_sample,
                                     float* out, int low_extinction, void* stream);
 
+/* DynamicProjectorExtension over a LinearDynamicVolume (projectors/dynamicprojectorextension.cpp:37-60,
+ * img/lineardynamicvolume.cpp:194-198): the reference re-projects each view with the voxels set to
+ * slope * float(t_view) + offset.  The projection is linear in the voxel values, so from the
+ * projections of the slope and the offset volumes over all views:
+ * out[view] = float(times[view]) * slope_proj[view] + offset_proj[view].
+ * times: n_views seconds, host memory; projections device memory, asynchronous on `stream`. */
+CTLCU_API int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* offset_proj,
+                                   const double* times, uint32_t n_views, uint64_t values_per_view, float* out,
+                                   void* stream);
+
 /*
  * No counterpart in the reference.  ctlcu_project for callers that cannot
  * allocate device memory while they run: a real-time loop that reserved all

@@ -122,3 +122,44 @@ def test_focal_spot_and_noise_follow_the_reference_test_strategy(ctx):
     diff = (mean - var) / mean
     assert abs(diff.mean()) < 0.05 and diff.std() < 0.25
     clean_ext.release()
+
+
+# ---- dynamic volumes ------------------------------------------------------------------------
+
+def _dynamic_case():
+    from ctl_b200 import geometry as G
+    from ctl_b200 import phantom as Ph
+    slope = Ph.ellipsoid_phantom((40, 40, 32), (2.0, 2.0, 2.0), 6, seed=31) * 0.5
+    offset = Ph.ellipsoid_phantom((40, 40, 32), (2.0, 2.0, 2.0), 6, seed=32)
+    P = G.circular_flat(6, 750.0, 1000.0, G.FlatDetector(48, 40, 2.0, 2.0))
+    times = [0.0, 0.25, 0.5, 1.0, 1.7, 3.0]
+    return slope, offset, P, times
+
+
+def test_linear_dynamic_volume_matches_the_reference_update():
+    """LinearDynamicVolume::updateVolume (img/lineardynamicvolume.cpp:194-198): slope * float(t) + offset."""
+    from ctl_b200.extensions import LinearDynamicVolume
+    slope, offset, _, _ = _dynamic_case()
+    d = LinearDynamicVolume(slope, offset, (2.0, 2.0, 2.0))
+    np.testing.assert_array_equal(d.at(1.7).data, slope * np.float32(1.7) + offset)
+
+
+@pytest.mark.gpu
+def test_dynamic_extension_matches_per_view_projection(ctx):
+    """Every view equals the oracle's projection of the volume at that view's time
+    (the reference's per-view loop), though it is computed by linearity from two
+    batched projections."""
+    from ctl_b200.extensions import DynamicProjectorExtension, LinearDynamicVolume
+    from ctl_b200.projector import VoxelVolume
+    slope, offset, P, times = _dynamic_case()
+    ext = DynamicProjectorExtension(ctx)
+    ext.configure(P, 48, 40, times)
+    dyn = LinearDynamicVolume(slope, offset, (2.0, 2.0, 2.0))
+    got = ext.project(dyn).cpu().numpy()
+    for v, t in enumerate(times):
+        want, _ = oracle.project_fp64(dyn.at(t).data, (2.0, 2.0, 2.0), P[v:v + 1], 48, 40)
+        assert rel_err(got[v:v + 1], want).max() <= TOL, v
+    # a volume that is not dynamic is projected as it is
+    plain = ext.project(VoxelVolume(offset, (2.0, 2.0, 2.0))).cpu().numpy()
+    want, _ = oracle.project_fp64(offset, (2.0, 2.0, 2.0), P, 48, 40)
+    assert rel_err(plain, want).max() <= TOL
