@@ -459,7 +459,8 @@ def run_postops(args):
     import torch
 
     from ctl_b200.projector import Context, Settings, VoxelVolume
-    vol, P = make_inputs()
+    n_views = args.views
+    vol, P = make_inputs(n_views)
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream)
     volume = ctx.volume(VoxelVolume(vol, VOXEL))
@@ -488,7 +489,7 @@ def run_postops(args):
         t0 = time.perf_counter()
         ctx.poisson_noise(h, i0, SEED_NOISE + i)
         e2e.append(time.perf_counter() - t0)
-    extra = {"e2e": {"value": N_VIEWS / statistics.mean(e2e), "unit": "projections/s",
+    extra = {"e2e": {"value": n_views / statistics.mean(e2e), "unit": "projections/s",
                      "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes),
                      "path": "ctlcu_poisson_noise on host data"},
              "gpu_launches": 1,
@@ -506,10 +507,10 @@ def run_postops(args):
         oracle.poisson_noise_reference(x, i0, SEED_NOISE)
         dt = time.perf_counter() - t0
         extra["cpu_baseline"] = {"value": sample / dt, "unit": "projections/s", "cores": 1, "kind": "port",
-                                 "sample": f"{sample} of {N_VIEWS} views with the reference's per-view "
+                                 "sample": f"{sample} of {n_views} views with the reference's per-view "
                                            f"mt19937_64 + std:: distributions, {dt:.2f} s"}
-    _line("projections/s through Poisson noise (PoissonNoiseExtension), 360 x 512^2, i0 = 1e4",
-          N_VIEWS / (t_ms / 1e3), "projections/s", t_ms, args,
+    _line(f"projections/s through Poisson noise (PoissonNoiseExtension), {n_views} x 512^2, i0 = 1e4",
+          n_views / (t_ms / 1e3), "projections/s", t_ms, args,
           {"workload": WORKLOAD + "; then Poisson noise, i0 = 1e4 photons/pixel"}, **extra)
     volume.release()
     ctx.close()

@@ -66,6 +66,25 @@ struct Stream {
 
 constexpr int kMaxRejections = 64;  // PTRS accepts > 85% of candidates; 64 rejections never occur
 
+// log(k!) for an integer k >= 0: the log of the exact product below 16 (15! < 2^53),
+// Stirling's series of log Gamma(x), x = k + 1, above:
+//   (x - 1/2) log x - x + log(2 pi)/2 + 1/(12x) - 1/(360x^3) + 1/(1260x^5) - 1/(1680x^7),
+// whose next term is below 1e-14 from x = 17 on.  It is cheap and branch-light: the
+// PTRS candidates that reach it are a few lanes of most warps.
+__device__ __forceinline__ double log_factorial(double k)
+{
+    if (k < 16.0) {
+        double p = 1.0;
+        for (int i = 2; i <= (int)k; ++i)
+            p *= (double)i;
+        return log(p);
+    }
+    const double x = k + 1.0;
+    const double r = 1.0 / x, r2 = r * r;
+    const double series = r * (1.0 / 12.0 - r2 * (1.0 / 360.0 - r2 * (1.0 / 1260.0 - r2 * (1.0 / 1680.0))));
+    return (x - 0.5) * log(x) - x + 0.91893853320467274178 + series;
+}
+
 // Poisson(lam) for 0 <= lam < 1e4, or Normal(lam, sqrt(lam)) for lam >= 1e4,
 // as the FP32 count the reference then takes the log of
 __device__ float noisy_count(double lam, Stream& s)
@@ -93,6 +112,7 @@ __device__ float noisy_count(double lam, Stream& s)
     const double a = -0.059 + 0.02483 * b;
     const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
     const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    const double log_inv_alpha = log(inv_alpha);
     for (int it = 0; it < kMaxRejections; ++it) {
         s.next(u, v);
         const double U = u - 0.5;
@@ -102,7 +122,7 @@ __device__ float noisy_count(double lam, Stream& s)
             return (float)k;
         if (k < 0.0 || (us < 0.013 && v > us))
             continue;
-        if (log(v) + log(inv_alpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0))
+        if (log(v) + log_inv_alpha - log(a / (us * us) + b) <= -lam + k * loglam - log_factorial(k))
             return (float)k;
     }
     return (float)floor(lam + 0.5);  // unreachable in practice (probability < 1e-50)

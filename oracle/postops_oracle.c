@@ -58,6 +58,22 @@ static void next2(stream_t* s, double* u, double* v)
     *v = u53(r.v[2], r.v[3]);
 }
 
+/* log(k!) as the device computes it: the exact product's log below 16, Stirling's
+ * series of log Gamma(k + 1) to the 1/(1680 x^7) term above. */
+static double log_factorial(double k)
+{
+    if (k < 16.0) {
+        double p = 1.0;
+        for (int i = 2; i <= (int)k; ++i)
+            p *= (double)i;
+        return log(p);
+    }
+    double x = k + 1.0;
+    double r = 1.0 / x, r2 = r * r;
+    double series = r * (1.0 / 12.0 - r2 * (1.0 / 360.0 - r2 * (1.0 / 1260.0 - r2 * (1.0 / 1680.0))));
+    return (x - 0.5) * log(x) - x + 0.91893853320467274178 + series;
+}
+
 static float noisy(double lam, stream_t* s)
 {
     double u, v;
@@ -81,6 +97,7 @@ static float noisy(double lam, stream_t* s)
     double a = -0.059 + 0.02483 * b;
     double ia = 1.1239 + 1.1328 / (b - 3.4);
     double vr = 0.9277 - 3.6224 / (b - 2.0);
+    double lia = log(ia);
     for (int it = 0; it < 64; ++it) {
         next2(s, &u, &v);
         double U = u - 0.5;
@@ -90,7 +107,7 @@ static float noisy(double lam, stream_t* s)
             return (float)k;
         if (k < 0.0 || (us < 0.013 && v > us))
             continue;
-        if (log(v) + log(ia) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0))
+        if (log(v) + lia - log(a / (us * us) + b) <= -lam + k * loglam - log_factorial(k))
             return (float)k;
     }
     return (float)floor(lam + 0.5);
