@@ -251,6 +251,34 @@ def test_batch_mixing_storage_types_matches_single_calls(ctx):
     vb.release()
 
 
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_PAIRS, L.KERNEL_GATHER], ids=["cells", "pairs", "gather"])
+def test_sub_rays_in_every_loop_match_oracle(ctx, kernel):
+    """raysPerPixel (3, 2) through the cell, pair and gather loops (the golden sub-ray
+    cases use up-sampling or nearest voxel, so they take other loops)."""
+    m, vol, P, _ = golden_cases()[5]   # anisotropic, off-centre, non-cubic; 40 x 36 detector
+    s = _settings(m, kernel=kernel)
+    s.rays_per_pixel = [3, 2]
+    gpu = ctx.project_volume(VoxelVolume(vol, m["voxel"], m["offset"]), P, m["channels"], m["rows"], s)
+    want, _ = oracle.project_fp64(vol, m["voxel"], P, m["channels"], m["rows"], offset_mm=m["offset"], rays=(3, 2))
+    assert rel_err(gpu, want).max() <= TOL
+
+
+def test_c3_full_size_512_cubed_helical_matches_oracle(ctx):
+    """512^3 (0.5 mm, a 4.4 GB cell array) -> two helical views of 64 curved modules of
+    16 x 16: the largest configuration, against the oracle."""
+    from ctl_b200 import workloads as W
+    P = W.c3_geometry()[[0, 719]]
+    vol = W.phantom_device((512, 512, 512), (0.5, 0.5, 0.5), 40, seed=3, texture=0.01, device="cuda")
+    v = ctx.volume(VoxelVolume(vol, (0.5, 0.5, 0.5)))
+    host = vol.cpu().numpy()
+    del vol
+    want, _ = oracle.project_fp64(host, (0.5, 0.5, 0.5), P, 16, 16)
+    for kernel in (L.KERNEL_CELLS, L.KERNEL_GATHER):
+        gpu = ctx.project(v, P, 16, 16, Settings(kernel=kernel))
+        assert rel_err(gpu, want).max() <= TOL, kernel
+    v.release()
+
+
 def test_cells_kernel_rejects_unsupported_settings(ctx):
     m, vol, P, _ = golden_cases()[0]
     for bad in (dict(interpolate=False), dict(volume_upsampling=2), dict(interp_mode=L.INTERP_TEXTURE)):
