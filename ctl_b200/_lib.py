@@ -127,6 +127,11 @@ SIGNATURES = [
     ("ctlcu_den_write", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                   C.c_uint32, C.c_void_p]),
     ("ctlcu_den_header", C.c_int, [C.c_char_p, C.POINTER(C.c_uint32 * 3), C.POINTER(C.c_uint32)]),
+    ("ctlcu_nrrd_write_projections", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                               C.c_uint32, C.c_uint32, C.c_void_p]),
+    ("ctlcu_nrrd_header", C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32 * 4), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    ("ctlcu_nrrd_read", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("ctlcu_den_read", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32,
                                  C.c_void_p]),
 ]

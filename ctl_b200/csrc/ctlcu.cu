@@ -1498,6 +1498,59 @@ int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t
     return r ? fail(ctx, r, "DEN write: %s", msg.c_str()) : CTLCU_OK;
 }
 
+int ctlcu_nrrd_write_projections(ctlcu_ctx* ctx, const char* path, const float* data, uint32_t n_views,
+                                 uint32_t n_modules, uint32_t rows, uint32_t channels, void* stream)
+{
+    std::string msg;
+    if (!ctx) {
+        if (!path || !data || is_device_ptr(data))
+            return CTLCU_ERR_INVALID_ARGUMENT;
+        return nrrd_write_projections(path, data, n_views, n_modules, rows, channels, nullptr, nullptr, msg);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!path || !data)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "path or data is NULL");
+    cudaSetDevice(ctx->device);
+    const int r = nrrd_write_projections(path, data, n_views, n_modules, rows, channels,
+                                         stream ? (cudaStream_t)stream : ctx->stream, &ctx->den, msg);
+    return r ? fail(ctx, r, "NRRD write: %s", msg.c_str()) : CTLCU_OK;
+}
+
+int ctlcu_nrrd_header(const char* path, uint32_t* version, uint32_t* n_dims, uint32_t sizes[4], uint32_t* elem_bytes,
+                      uint64_t* data_offset)
+{
+    if (!path || !version || !n_dims || !sizes || !elem_bytes || !data_offset)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    NrrdHeader h;
+    std::string msg;
+    const int r = nrrd_header(path, h, msg);
+    if (r)
+        return r;
+    *version = h.version;
+    *n_dims = h.n_dims;
+    for (int k = 0; k < 4; ++k)
+        sizes[k] = h.sizes[k];
+    *elem_bytes = h.elem;
+    *data_offset = h.offset;
+    return CTLCU_OK;
+}
+
+int ctlcu_nrrd_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, void* stream)
+{
+    std::string msg;
+    if (!ctx) {
+        if (!path || !data || is_device_ptr(data))
+            return CTLCU_ERR_INVALID_ARGUMENT;
+        return nrrd_read(path, data, capacity_bytes, nullptr, nullptr, msg);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!path || !data)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "path or data is NULL");
+    cudaSetDevice(ctx->device);
+    const int r = nrrd_read(path, data, capacity_bytes, stream ? (cudaStream_t)stream : ctx->stream, &ctx->den, msg);
+    return r ? fail(ctx, r, "NRRD read: %s", msg.c_str()) : CTLCU_OK;
+}
+
 int ctlcu_den_header(const char* path, uint32_t dims[3], uint32_t* elem_bytes)
 {
     if (!path || !dims || !elem_bytes)

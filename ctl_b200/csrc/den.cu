@@ -92,43 +92,80 @@ int den_write(const char* path, const void* data, uint32_t elem, uint32_t rows, 
     }
     const uint16_t head[3] = { (uint16_t)rows, (uint16_t)cols, (uint16_t)count };
     const size_t total = (size_t)rows * cols * count * elem;
-    bool ok = std::fwrite(head, 1, 6, f) == 6;
-    if (ok && (!stage || !is_device(data))) {
-        ok = std::fwrite(data, 1, total, f) == total;
-    } else if (ok) {
-        DenStaging& s = *stage;
-        cudaError_t e = s.ensure();
-        const char* src = static_cast<const char*>(data);
-        const size_t n = (total + kStage - 1) / kStage;
-        auto issue = [&](size_t i) {
-            const size_t off = i * kStage, len = std::min(kStage, total - off);
-            cudaError_t r = cudaMemcpyAsync(s.buf[i & 1], src + off, len, cudaMemcpyDeviceToHost, st);
-            return r == cudaSuccess ? cudaEventRecord(s.ev[i & 1], st) : r;
-        };
-        if (e == cudaSuccess)
-            e = issue(0);
-        for (size_t i = 0; e == cudaSuccess && ok && i < n; ++i) {
-            if (i + 1 < n)
-                e = issue(i + 1);  // its buffer was written out in iteration i - 1
-            if (e == cudaSuccess)
-                e = cudaEventSynchronize(s.ev[i & 1]);
-            const size_t len = std::min(kStage, total - i * kStage);
-            if (e == cudaSuccess)
-                ok = std::fwrite(s.buf[i & 1], 1, len, f) == len;
-        }
-        if (e != cudaSuccess) {
-            cudaStreamSynchronize(st);
-            std::fclose(f);
-            msg = std::string("device copy: ") + cudaGetErrorString(e);
-            return CTLCU_ERR_CUDA;
-        }
-    }
-    ok = (std::fclose(f) == 0) && ok;
-    if (!ok) {
+    int r = std::fwrite(head, 1, 6, f) == 6 ? file_write_data(f, data, total, st, stage, msg)
+                                            : CTLCU_ERR_INVALID_ARGUMENT;
+    const bool closed = std::fclose(f) == 0;
+    if (r == CTLCU_OK && !closed)
+        r = CTLCU_ERR_INVALID_ARGUMENT;
+    if (r == CTLCU_ERR_INVALID_ARGUMENT && msg.empty())
         msg = std::string("writing ") + path + " failed";
-        return CTLCU_ERR_INVALID_ARGUMENT;
+    return r;
+}
+
+int file_write_data(FILE* f, const void* data, size_t total, cudaStream_t st, DenStaging* stage, std::string& msg)
+{
+    if (!stage || !is_device(data))
+        return std::fwrite(data, 1, total, f) == total ? CTLCU_OK : CTLCU_ERR_INVALID_ARGUMENT;
+    DenStaging& s = *stage;
+    cudaError_t e = s.ensure();
+    const char* src = static_cast<const char*>(data);
+    const size_t n = (total + kStage - 1) / kStage;
+    auto issue = [&](size_t i) {
+        const size_t off = i * kStage, len = std::min(kStage, total - off);
+        cudaError_t r = cudaMemcpyAsync(s.buf[i & 1], src + off, len, cudaMemcpyDeviceToHost, st);
+        return r == cudaSuccess ? cudaEventRecord(s.ev[i & 1], st) : r;
+    };
+    bool ok = true;
+    if (e == cudaSuccess && n > 0)
+        e = issue(0);
+    for (size_t i = 0; e == cudaSuccess && ok && i < n; ++i) {
+        if (i + 1 < n)
+            e = issue(i + 1);  // its buffer was written out in iteration i - 1
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(s.ev[i & 1]);
+        const size_t len = std::min(kStage, total - i * kStage);
+        if (e == cudaSuccess)
+            ok = std::fwrite(s.buf[i & 1], 1, len, f) == len;
     }
-    return CTLCU_OK;
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        msg = std::string("device copy: ") + cudaGetErrorString(e);
+        return CTLCU_ERR_CUDA;
+    }
+    return ok ? CTLCU_OK : CTLCU_ERR_INVALID_ARGUMENT;
+}
+
+int file_read_data(FILE* f, void* data, size_t total, cudaStream_t st, DenStaging* stage, std::string& msg)
+{
+    if (!stage || !is_device(data))
+        return std::fread(data, 1, total, f) == total ? CTLCU_OK : CTLCU_ERR_INVALID_ARGUMENT;
+    DenStaging& s = *stage;
+    cudaError_t e = s.ensure();
+    char* dst = static_cast<char*>(data);
+    const size_t n = (total + kStage - 1) / kStage;
+    bool ok = true;
+    for (size_t i = 0; e == cudaSuccess && ok && i < n; ++i) {
+        const size_t off = i * kStage, len = std::min<uint64_t>(kStage, total - off);
+        if (i >= 2)
+            e = cudaEventSynchronize(s.ev[i & 1]);  // the copy out of this buffer is done
+        if (e != cudaSuccess)
+            break;
+        ok = std::fread(s.buf[i & 1], 1, len, f) == len;
+        if (ok)
+            e = cudaMemcpyAsync(dst + off, s.buf[i & 1], len, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(s.ev[i & 1], st);
+    }
+    // the data is in place, and the staging buffers free for the next call, once
+    // the copies out of them are done
+    const cudaError_t w = cudaStreamSynchronize(st);
+    if (e == cudaSuccess)
+        e = w;
+    if (e != cudaSuccess) {
+        msg = std::string("device copy: ") + cudaGetErrorString(e);
+        return CTLCU_ERR_CUDA;
+    }
+    return ok ? CTLCU_OK : CTLCU_ERR_INVALID_ARGUMENT;
 }
 
 int den_header(const char* path, uint32_t dims[3], uint32_t* elem, std::string& msg)
@@ -192,43 +229,11 @@ int den_read(const char* path, void* data, uint64_t capacity, uint32_t first, ui
         msg = std::string("cannot read ") + path;
         return CTLCU_ERR_INVALID_ARGUMENT;
     }
-    bool ok = true;
-    if (!stage || !is_device(data)) {
-        ok = std::fread(data, 1, total, f) == total;
-    } else {
-        DenStaging& s = *stage;
-        cudaError_t e = s.ensure();
-        char* dst = static_cast<char*>(data);
-        const size_t n = (total + kStage - 1) / kStage;
-        for (size_t i = 0; e == cudaSuccess && ok && i < n; ++i) {
-            const size_t off = i * kStage, len = std::min<uint64_t>(kStage, total - off);
-            if (i >= 2)
-                e = cudaEventSynchronize(s.ev[i & 1]);  // the copy out of this buffer is done
-            if (e != cudaSuccess)
-                break;
-            ok = std::fread(s.buf[i & 1], 1, len, f) == len;
-            if (ok)
-                e = cudaMemcpyAsync(dst + off, s.buf[i & 1], len, cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess)
-                e = cudaEventRecord(s.ev[i & 1], st);
-        }
-        // the data is in place, and the staging buffers free for the next call, once
-        // the copies out of them are done
-        const cudaError_t w = cudaStreamSynchronize(st);
-        if (e == cudaSuccess)
-            e = w;
-        if (e != cudaSuccess) {
-            std::fclose(f);
-            msg = std::string("device copy: ") + cudaGetErrorString(e);
-            return CTLCU_ERR_CUDA;
-        }
-    }
+    const int rd = file_read_data(f, data, total, st, stage, msg);
     std::fclose(f);
-    if (!ok) {
+    if (rd == CTLCU_ERR_INVALID_ARGUMENT && msg.empty())
         msg = std::string("reading ") + path + " failed";
-        return CTLCU_ERR_INVALID_ARGUMENT;
-    }
-    return CTLCU_OK;
+    return rd;
 }
 
 }  // namespace ctlcu

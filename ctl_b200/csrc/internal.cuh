@@ -247,6 +247,7 @@ cudaError_t launch_transform(float* data, uint64_t per_view, uint32_t n_views, c
                              cudaStream_t s);
 }  // namespace ctlcu
 
+#include <cstdio>
 #include <string>
 
 namespace ctlcu {
@@ -264,5 +265,19 @@ int den_write(const char* path, const void* data, uint32_t elem, uint32_t rows, 
 int den_header(const char* path, uint32_t dims[3], uint32_t* elem, std::string& msg);
 int den_read(const char* path, void* data, uint64_t capacity, uint32_t first, uint32_t n_mats, cudaStream_t st,
              DenStaging* stage, std::string& msg);
+// Write / read `total` bytes of host or device data at an open file's position
+// (device data through the staging buffers, copies overlapping the file I/O).
+int file_write_data(FILE* f, const void* data, size_t total, cudaStream_t st, DenStaging* stage, std::string& msg);
+int file_read_data(FILE* f, void* data, size_t total, cudaStream_t st, DenStaging* stage, std::string& msg);
+struct NrrdHeader {
+    uint32_t version = 0, n_dims = 0, sizes[4] = { 0, 0, 0, 0 };
+    uint32_t elem = 0;       // bytes per element
+    bool is_float = false;   // float/double (else integer)
+    uint64_t offset = 0;     // bytes before the data
+};
+int nrrd_header(const char* path, NrrdHeader& h, std::string& msg);
+int nrrd_write_projections(const char* path, const float* data, uint32_t views, uint32_t modules, uint32_t rows,
+                           uint32_t channels, cudaStream_t st, DenStaging* stage, std::string& msg);
+int nrrd_read(const char* path, void* data, uint64_t capacity, cudaStream_t st, DenStaging* stage, std::string& msg);
 
 }  // namespace ctlcu

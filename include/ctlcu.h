@@ -282,6 +282,26 @@ CTLCU_API int ctlcu_den_header(const char* path, uint32_t dims[3], uint32_t* ele
 CTLCU_API int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, uint32_t first,
                              uint32_t n, void* stream);
 
+/* ---- NRRD files --------------------------------------------------------------------------- */
+
+/* BaseTypeIO<NrrdFileIO>::write(ProjectionData) (io/basetypeio.tpp:342-362,
+ * io/nrrd/nrrdfileio.tpp:221-337): the header CTL writes for projections
+ * (NRRD0004, float, dimension 4, sizes channels rows modules views, their labels,
+ * raw little-endian, "type hint:=projection data") and the data [view][module][row][channel]
+ * from device memory (streamed through pinned staging) or host memory (ctx may be NULL). */
+CTLCU_API int ctlcu_nrrd_write_projections(ctlcu_ctx* ctx, const char* path, const float* data, uint32_t n_views,
+                                           uint32_t n_modules, uint32_t rows, uint32_t channels, void* stream);
+
+/* NrrdFileIO::metaInfo (io/nrrd/nrrdfileio.tpp:20-105, :352-450): the header's version,
+ * dimension and sizes (fastest first), element bytes and the offset of the data.
+ * Comments and key-value pairs are skipped; only raw little-endian data is accepted. */
+CTLCU_API int ctlcu_nrrd_header(const char* path, uint32_t* version, uint32_t* n_dims, uint32_t sizes[4],
+                                uint32_t* elem_bytes, uint64_t* data_offset);
+
+/* NrrdFileIO::readAll: the whole data block into `data` (device memory, through pinned
+ * staging, or host memory; ctx may be NULL for host memory) of capacity_bytes. */
+CTLCU_API int ctlcu_nrrd_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, void* stream);
+
 /* ---- geometry encoding ------------------------------------------------------------------- */
 
 /* Detector of a simple CT system: CylindricalDetector(nbPixelPerModule,

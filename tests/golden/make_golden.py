@@ -20,6 +20,7 @@ Writes
                    oracle/ref_harness.cpp)
   den_files.json   size, header and SHA-256 of testing/testData/tubeGeo.den and
                    cArmGeo.den (the DEN writer must reproduce them byte for byte)
+  header.nrrd      testing/testData/header.nrrd, the reference's NRRD header test file
 """
 from __future__ import annotations
 
@@ -108,6 +109,9 @@ def den_files():
                      "sha256": hashlib.sha256(raw).hexdigest()}
     with open(os.path.join(HERE, "den_files.json"), "w") as f:
         json.dump(out, f, indent=1)
+    # the reference's NRRD reader test file (testing/src/nrrdfileiotest.cpp:6), copied as it is
+    with open(os.path.join(TESTDATA, "header.nrrd"), "rb") as src, open(os.path.join(HERE, "header.nrrd"), "wb") as dst:
+        dst.write(src.read())
 
 
 if __name__ == "__main__":
