@@ -1452,6 +1452,62 @@ int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, u
     return CTLCU_OK;
 }
 
+int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs, uint32_t n_materials, uint32_t n_views,
+                           uint64_t values_per_view, const float* mu_per_mm, const double* intensities,
+                           const float* response, uint32_t n_bins, const double* total_intensity, float* out,
+                           void* stream)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!material_projs || !mu_per_mm || !intensities || !total_intensity || !out || !n_materials || !n_bins)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "NULL argument, no materials or no energy bins");
+    if (n_views == 0 || values_per_view == 0)
+        return CTLCU_OK;
+    cudaSetDevice(ctx->device);
+    if (!is_device_ptr(material_projs) || !is_device_ptr(out))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "projections must be device memory");
+    // spectraleffectsextension.cpp:339: a bin whose intensities sum to (fuzzy) zero is skipped
+    std::vector<int> skip(n_bins, 0);
+    for (uint32_t b = 0; b < n_bins; ++b) {
+        double s = 0.0;
+        for (uint32_t v = 0; v < n_views; ++v)
+            s += intensities[(size_t)b * n_views + v];
+        skip[b] = std::fabs(s) <= 1e-12;
+    }
+    std::vector<float> resp(n_bins, 1.0f);
+    if (response)
+        std::copy(response, response + n_bins, resp.begin());
+    const size_t b_mu = sizeof(float) * n_bins * n_materials, b_int = sizeof(double) * n_bins * n_views,
+                 b_resp = sizeof(float) * n_bins, b_skip = sizeof(int) * n_bins, b_tot = sizeof(double) * n_views;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    char* buf = nullptr;
+    const size_t o_int = 0, o_tot = o_int + b_int, o_mu = o_tot + b_tot, o_resp = o_mu + b_mu, o_skip = o_resp + b_resp;
+    CU_TRY(ctx, cudaMallocAsync((void**)&buf, o_skip + b_skip, st));
+    cudaError_t e = cudaMemcpyAsync(buf + o_int, intensities, b_int, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf + o_tot, total_intensity, b_tot, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf + o_mu, mu_per_mm, b_mu, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf + o_resp, resp.data(), b_resp, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf + o_skip, skip.data(), b_skip, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = launch_spectral(material_projs, n_materials, values_per_view, n_views, (const float*)(buf + o_mu),
+                            (const double*)(buf + o_int), (const float*)(buf + o_resp), (const int*)(buf + o_skip),
+                            n_bins, (const double*)(buf + o_tot), out, st);
+    // the host vectors die on return: the copies out of them must be done
+    const cudaError_t w = cudaStreamSynchronize(st);
+    cudaFreeAsync(buf, st);
+    if (e == cudaSuccess)
+        e = w;
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "spectral combine: %s", cudaGetErrorString(e));
+    ++ctx->launches;
+    return CTLCU_OK;
+}
+
 int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* offset_proj, const double* times,
                          uint32_t n_views, uint64_t values_per_view, float* out, void* stream)
 {

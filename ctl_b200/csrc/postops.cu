@@ -192,6 +192,35 @@ __global__ void combine_kernel(const float* __restrict__ slope, const float* __r
     }
 }
 
+// SpectralEffectsExtension::projectLinear / singleBinIntensityLinear
+// (projectors/spectraleffectsextension.cpp:215-278, :333-353), per pixel of view v,
+// in FP32 like the reference:
+//   sum = sum over bins b with non-zero intensity of
+//         float(intensity[b][v]) * exp(-(sum over materials m of proj[m] * mu[b][m])) * response[b]
+//   out = log(float(total[v]) / sum)
+// proj: [material][n], n = views x values per view; mu: [bin][material] (1/mm);
+// intensity: [bin][view]; response: [bin] (1 without a detector response model).
+__global__ void spectral_kernel(const float* __restrict__ proj, uint32_t n_materials, uint64_t per_view,
+                                uint32_t n_views, const float* __restrict__ mu, const double* __restrict__ intensity,
+                                const float* __restrict__ response, const int* __restrict__ skip, uint32_t n_bins,
+                                const double* __restrict__ total, float* __restrict__ out)
+{
+    const uint64_t n = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(i / per_view);
+        float sum = 0.0f;
+        for (uint32_t b = 0; b < n_bins; ++b) {
+            if (skip[b])
+                continue;
+            float e = 0.0f;
+            for (uint32_t m = 0; m < n_materials; ++m)
+                e += proj[(uint64_t)m * n + i] * mu[(uint64_t)b * n_materials + m];
+            sum += (float)intensity[(uint64_t)b * n_views + v] * expf(-e) * response[b];
+        }
+        out[i] = logf((float)total[v] / sum);
+    }
+}
+
 unsigned grid_for_elements(uint64_t n)
 {
     uint64_t b = (n + 255) / 256;
@@ -209,6 +238,18 @@ cudaError_t launch_poisson_noise(float* data, uint32_t n_views, uint32_t n_modul
         return cudaSuccess;
     poisson_kernel<<<grid_for_elements(total), 256, 0, s>>>(data, n_views, n_modules, ppm, i0, (uint32_t)seed,
                                                              (uint32_t)(seed >> 32));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spectral(const float* proj, uint32_t n_materials, uint64_t per_view, uint32_t n_views,
+                            const float* mu, const double* intensity, const float* response, const int* skip,
+                            uint32_t n_bins, const double* total, float* out, cudaStream_t s)
+{
+    const uint64_t n = per_view * n_views;
+    if (n == 0)
+        return cudaSuccess;
+    spectral_kernel<<<grid_for_elements(n), 256, 0, s>>>(proj, n_materials, per_view, n_views, mu, intensity, response,
+                                                          skip, n_bins, total, out);
     return cudaGetLastError();
 }
 

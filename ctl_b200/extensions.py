@@ -184,6 +184,68 @@ class DynamicProjectorExtension:
             vo.release()
 
 
+class SpectralEffectsExtension:
+    """SpectralEffectsExtension, linear case (projectors/spectraleffectsextension.cpp:215-278):
+    the materials' density volumes projected in one batched launch, then every energy bin
+    combined per pixel on the device (ctlcu_spectral_combine).
+
+    The spectral inputs come from CTL's models, evaluated by the caller:
+      mu_per_mm  [bins][materials]: meanMassAttenuationCoeff(E_b, binWidth) * 0.1 (cm -> mm)
+      intensities [bins][views]:   RadiationEncoder bin intensities per view
+      total_intensity [views]:     RadiationEncoder::totalIntensity()
+      response [bins] or None:     the detector's spectral response model at E_b"""
+
+    def __init__(self, ctx: Context, settings: Optional[Settings] = None):
+        self.ctx = ctx
+        self.settings = settings or Settings()
+        self._pm = None
+
+    def configure(self, pmats, channels: int, rows: int, mu_per_mm, intensities, total_intensity,
+                  response=None) -> None:
+        self._pm = pmats
+        self._dims = (int(channels), int(rows))
+        self.mu = np.ascontiguousarray(mu_per_mm, np.float32)
+        self.intensities = np.ascontiguousarray(intensities, np.float64)
+        self.total = np.ascontiguousarray(total_intensity, np.float64)
+        self.response = None if response is None else np.ascontiguousarray(response, np.float32)
+        B, M = self.mu.shape
+        V = int(pmats.shape[0])
+        if self.intensities.shape != (B, V) or self.total.shape != (V,):
+            raise ValueError("intensities must be [bins][views] and total_intensity [views]")
+        if self.response is not None and self.response.shape != (B,):
+            raise ValueError("response must hold one value per bin")
+
+    def project(self, material_densities: Sequence[VoxelVolume]):
+        import torch
+        if self._pm is None:
+            raise RuntimeError("SpectralEffectsExtension::project: configure() has not been called")
+        C_, R = self._dims
+        M = len(material_densities)
+        if M != self.mu.shape[1]:
+            raise ValueError("one mass attenuation column per material")
+        P = self._pm if hasattr(self._pm, "is_cuda") else torch.from_numpy(np.ascontiguousarray(self._pm)).cuda()
+        V, Mod = int(P.shape[0]), int(P.shape[1])
+        vols = [self.ctx.volume(v, self.settings.storage) for v in material_densities]
+        try:
+            projs = torch.empty((M, V, Mod, R, C_), dtype=torch.float32, device="cuda")
+            self.ctx.project_batch([(vol, P, projs[m]) for m, vol in enumerate(vols)], self.settings)
+            out = torch.empty((V, Mod, R, C_), dtype=torch.float32, device="cuda")
+            from .projector import _ptr
+            import ctypes as C
+            stream = self.ctx._stream_for(0, out)
+            self.ctx._check(self.ctx.lib.ctlcu_spectral_combine(
+                self.ctx.h, C.c_void_p(_ptr(projs)), M, V, Mod * R * C_, C.c_void_p(self.mu.ctypes.data),
+                C.c_void_p(self.intensities.ctypes.data),
+                C.c_void_p(self.response.ctypes.data if self.response is not None else None),
+                int(self.mu.shape[0]), C.c_void_p(self.total.ctypes.data), C.c_void_p(_ptr(out)),
+                C.c_void_p(stream or None)))
+            return out
+        finally:
+            torch.cuda.synchronize()
+            for vol in vols:
+                vol.release()
+
+
 class PoissonNoiseExtension:
     """PoissonNoiseExtension around a B200 projector or extension (anything with
     project(volume) returning device extinctions [views, modules, rows, channels]).

@@ -383,6 +383,20 @@ CTLCU_API int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, cons
                                    const double* times, uint32_t n_views, uint64_t values_per_view, float* out,
                                    void* stream);
 
+/* SpectralEffectsExtension, linear case (projectors/spectraleffectsextension.cpp:215-278,
+ * :333-353): from the projections of the materials' density volumes
+ * (material_projs [material][view][...], device), per pixel of view v
+ *   out = log(total_intensity[v] / sum_b intensities[b][v] exp(-sum_m mu_per_mm[b][m] proj_m) response[b])
+ * in FP32 as the reference computes it; bins whose intensities sum to zero are skipped.
+ * mu_per_mm [bin][material] (mass attenuation x 0.1, cm -> mm), intensities [bin][view],
+ * response [bin] (NULL: no detector response model) and total_intensity [view] are
+ * host memory, from CTL's spectral models (RadiationEncoder, attenuation models).
+ * out: device; returns when done. */
+CTLCU_API int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs, uint32_t n_materials,
+                                     uint32_t n_views, uint64_t values_per_view, const float* mu_per_mm,
+                                     const double* intensities, const float* response, uint32_t n_bins,
+                                     const double* total_intensity, float* out, void* stream);
+
 /*
  * No counterpart in the reference.  ctlcu_project for callers that cannot
  * allocate device memory while they run: a real-time loop that reserved all

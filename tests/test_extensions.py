@@ -124,6 +124,41 @@ def test_focal_spot_and_noise_follow_the_reference_test_strategy(ctx):
     clean_ext.release()
 
 
+# ---- spectral effects -----------------------------------------------------------------------
+
+@pytest.mark.gpu
+def test_spectral_extension_matches_the_oracle(ctx):
+    """Two material densities, four energy bins (one with zero intensity, which the
+    reference skips), per-view intensities and a detector response: one batched
+    projection of the materials and the device combine, against per-material oracle
+    projections combined in FP64 (spectraleffectsextension.cpp:215-278, :333-353)."""
+    from ctl_b200 import geometry as G
+    from ctl_b200 import phantom as Ph
+    from ctl_b200.extensions import SpectralEffectsExtension
+    from ctl_b200.projector import VoxelVolume
+    vox = (2.0, 2.0, 2.0)
+    water = Ph.ellipsoid_phantom((40, 40, 32), vox, 5, seed=41) * 40.0   # densities, g/cm^3
+    bone = Ph.ellipsoid_phantom((40, 40, 32), vox, 3, seed=42) * 20.0
+    P = G.circular_flat(5, 750.0, 1000.0, G.FlatDetector(48, 40, 2.0, 2.0))
+    mu = np.array([[0.0268, 0.0573], [0.0206, 0.0303], [0.0, 0.0], [0.0184, 0.0223]], np.float32)  # 1/mm per g/cm^3
+    rng = np.random.default_rng(5)
+    inten = rng.uniform(100.0, 1000.0, (4, 5))
+    inten[2] = 0.0                          # an empty bin
+    response = np.array([0.9, 0.95, 1.0, 0.8], np.float32)
+    total = inten.sum(0)
+    ext = SpectralEffectsExtension(ctx)
+    ext.configure(P, 48, 40, mu, inten, total, response)
+    got = ext.project([VoxelVolume(water, vox), VoxelVolume(bone, vox)]).cpu().numpy()
+    pw, _ = oracle.project_fp64(water, vox, P, 48, 40)
+    pb, _ = oracle.project_fp64(bone, vox, P, 48, 40)
+    acc = np.zeros(pw.shape)
+    for b in (0, 1, 3):
+        e = pw.astype(np.float64) * mu[b, 0] + pb.astype(np.float64) * mu[b, 1]
+        acc += inten[b][:, None, None, None] * np.exp(-e) * response[b]
+    want = np.log(total[:, None, None, None] / acc)
+    assert rel_err(got, want).max() <= TOL
+
+
 # ---- dynamic volumes ------------------------------------------------------------------------
 
 def _dynamic_case():
