@@ -960,6 +960,7 @@ int ctlcu_stream(ctlcu_ctx* ctx, void** stream)
 int ctlcu_volume_create(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const float* data,
                         int data_on_device, uint64_t* handle)
 {
+    TraceRange trace_("ctlcu_volume_create");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1028,6 +1029,7 @@ int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* setting
                   uint32_t n_views, uint32_t n_modules, uint32_t channels, uint32_t rows, float* out,
                   void* stream)
 {
+    TraceRange trace_("ctlcu_project");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1051,6 +1053,7 @@ int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const fl
                          const ctlcu_settings* settings, const double* pmats, uint32_t n_views,
                          uint32_t n_modules, uint32_t channels, uint32_t rows, float* out)
 {
+    TraceRange trace_("ctlcu_project_volume");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1080,6 +1083,7 @@ int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const fl
 int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
                         const ctlcu_settings* settings, void* stream)
 {
+    TraceRange trace_("ctlcu_project_batch");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1194,6 +1198,7 @@ int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_
 
 int ctlcu_plan_launch(ctlcu_plan* plan, void* stream)
 {
+    TraceRange trace_("ctlcu_plan_launch");
     if (!plan)
         return CTLCU_ERR_INVALID_ARGUMENT;
     ctlcu_ctx* ctx = plan->ctx;
@@ -1296,6 +1301,7 @@ int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settin
                    uint32_t n_views, uint32_t n_modules, uint32_t channels, uint32_t rows, uint32_t max_views,
                    int* kernel_out, float* ms_out)
 {
+    TraceRange trace_("ctlcu_autotune");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1438,6 +1444,7 @@ int ctlcu_launch_count(ctlcu_ctx* ctx, uint64_t* launches)
 int ctlcu_average_samples(ctlcu_ctx* ctx, const float* in, uint32_t n_samples, uint64_t values_per_sample,
                           float* out, int low_extinction, void* stream)
 {
+    TraceRange trace_("ctlcu_average_samples");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1457,6 +1464,7 @@ int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs, uint32_t
                            const float* response, uint32_t n_bins, const double* total_intensity, float* out,
                            void* stream)
 {
+    TraceRange trace_("ctlcu_spectral_combine");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1511,6 +1519,7 @@ int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs, uint32_t
 int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* offset_proj, const double* times,
                          uint32_t n_views, uint64_t values_per_view, float* out, void* stream)
 {
+    TraceRange trace_("ctlcu_combine_linear");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1537,6 +1546,7 @@ int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* o
 int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t elem_bytes, uint32_t rows,
                     uint32_t cols, uint32_t count, void* stream)
 {
+    TraceRange trace_("ctlcu_den_write");
     if (!ctx) {
         // host data needs no context (nor a GPU)
         if (!path || !data || is_device_ptr(data))
@@ -1557,6 +1567,7 @@ int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t
 int ctlcu_nrrd_write_projections(ctlcu_ctx* ctx, const char* path, const float* data, uint32_t n_views,
                                  uint32_t n_modules, uint32_t rows, uint32_t channels, void* stream)
 {
+    TraceRange trace_("ctlcu_nrrd_write_projections");
     std::string msg;
     if (!ctx) {
         if (!path || !data || is_device_ptr(data))
@@ -1593,6 +1604,7 @@ int ctlcu_nrrd_header(const char* path, uint32_t* version, uint32_t* n_dims, uin
 
 int ctlcu_nrrd_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, void* stream)
 {
+    TraceRange trace_("ctlcu_nrrd_read");
     std::string msg;
     if (!ctx) {
         if (!path || !data || is_device_ptr(data))
@@ -1618,6 +1630,7 @@ int ctlcu_den_header(const char* path, uint32_t dims[3], uint32_t* elem_bytes)
 int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capacity_bytes, uint32_t first, uint32_t n,
                    void* stream)
 {
+    TraceRange trace_("ctlcu_den_read");
     if (!ctx) {
         if (!path || !data || is_device_ptr(data))
             return CTLCU_ERR_INVALID_ARGUMENT;
@@ -1637,18 +1650,21 @@ int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capaci
 int ctlcu_transform_to_extinction(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
                                   const double* i0, void* stream)
 {
+    TraceRange trace_("ctlcu_transform_to_extinction");
     return transform(ctx, data, n_views, values_per_view, i0, stream, true);
 }
 
 int ctlcu_transform_to_intensity(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint64_t values_per_view,
                                  const double* i0, void* stream)
 {
+    TraceRange trace_("ctlcu_transform_to_intensity");
     return transform(ctx, data, n_views, values_per_view, i0, stream, false);
 }
 
 int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t n_modules, uint32_t pixels_per_module,
                         const float* i0_per_module, uint64_t seed, void* stream)
 {
+    TraceRange trace_("ctlcu_poisson_noise");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1690,6 +1706,7 @@ int ctlcu_encode_geometry_shifted(ctlcu_ctx* ctx, const ctlcu_detector_desc* det
                                   const ctlcu_trajectory_desc* trajectory, uint32_t n_views,
                                   const double* source_shifts_mm, uint32_t n_shifts, double* pmats, void* stream)
 {
+    TraceRange trace_("ctlcu_encode_geometry_shifted");
     if (!ctx)
         return CTLCU_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lk(ctx->mu);

@@ -253,7 +253,18 @@ cudaError_t launch_transform(float* data, uint64_t per_view, uint32_t n_views, c
 #include <cstdio>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace ctlcu {
+// A named NVTX range around a C-ABI call, for timeline tools (Nsight Systems,
+// Nsight Compute's --nvtx filters); a no-op when no tool is attached.
+struct TraceRange {
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
+
 // Two pinned host buffers and their events for streaming device data to and
 // from files; a context keeps one, allocated on first use.
 struct DenStaging {
