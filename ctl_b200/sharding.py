@@ -30,6 +30,26 @@ def project_shard(project: Callable[[np.ndarray], object], pmats, world: int, ra
     return start, stop, project(pmats[start:stop])
 
 
+def broadcast_volume(volume, shape, src: int = 0, device=None, group=None):
+    """The volume on every rank from rank `src` (the only rank that needs to read or
+    generate it): one broadcast, over NVLink with NCCL on GPUs, in place of each rank
+    loading its own copy (the reference uploads it to every device from the host,
+    raycasterprojector.cpp:239-251).  `volume` is ignored on the other ranks."""
+    import torch
+    import torch.distributed as dist
+    rank = dist.get_rank(group)
+    if rank == src:
+        t = torch.as_tensor(volume, dtype=torch.float32)
+        t = t.to(device) if device is not None else t
+        t = t.contiguous()
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"volume has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    else:
+        t = torch.empty(tuple(shape), dtype=torch.float32, device=device)
+    dist.broadcast(t, src=src, group=group)
+    return t
+
+
 def gather_views(local, n_views: int, world: int, rank: int, group=None):
     """All-gather the per-rank view slices into the full [view][...] tensor."""
     import torch
