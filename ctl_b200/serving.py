@@ -73,7 +73,7 @@ class ServeStats:
 class DRRServer:
     def __init__(self, ctx: Context, volumes: Sequence[Volume], channels: int, rows: int,
                  settings: Optional[Settings] = None, streams: int = 2, max_batch: int = 256,
-                 budget_bytes: int = 40 * 10**9, refuse: bool = False):
+                 budget_bytes: int = 40 * 10**9, refuse: bool = False, deadline_ms: Optional[float] = None):
         import torch
         self.torch = torch
         self.ctx = ctx
@@ -83,6 +83,9 @@ class DRRServer:
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.max_batch = max_batch
         self.refuse = refuse
+        # a queued request that has waited longer than this when a stream frees is
+        # refused rather than served late
+        self.deadline_s = None if deadline_ms is None else deadline_ms / 1e3
         self.budget_bytes = budget_bytes
         if self._free_budget() <= 0:
             raise ValueError("the resident volumes alone exceed the memory budget")
@@ -159,6 +162,17 @@ class DRRServer:
                         used -= self._bytes(r)
                     done += len(slot[0])
                     inflight[i] = None
+                if inflight[i] is None and queue and self.deadline_s is not None:
+                    late = time.perf_counter() - t0 - self.deadline_s
+                    kept = []
+                    for r in queue:
+                        if r.arrival < late:
+                            r.refused = True
+                            refused += 1
+                            used -= self._bytes(r)
+                        else:
+                            kept.append(r)
+                    queue = kept
                 if inflight[i] is None and queue:
                     batch, queue = queue[: self.max_batch], queue[self.max_batch:]
                     with torch.cuda.stream(s):

@@ -64,3 +64,20 @@ def test_server_admission_by_budget():
         DRRServer(ctx, [h], 48, 40, budget_bytes=1)
     h.release()
     ctx.close()
+
+
+def test_server_deadline_refuses_late_requests():
+    """Far above capacity with a short deadline: requests that waited longer than the
+    deadline when a stream freed are refused, and every served request started in time."""
+    ctx = Context(0)
+    vol = Ph.ellipsoid_phantom((64, 64, 64), (2, 2, 2), 5, seed=2)
+    h = ctx.volume(VoxelVolume(vol, (2, 2, 2)))
+    server = DRRServer(ctx, [h], 48, 40, Settings(), streams=1, max_batch=2, deadline_ms=2.0)
+    server.warm_up()
+    reqs = poisson_requests(1e6, 400, 1, _base_view(), seed=5, views=(16, 16))
+    stats = server.run(reqs)
+    assert stats.refused > 0 and stats.completed > 0 and stats.completed + stats.refused == 400
+    served = [r for r in reqs if not r.refused]
+    assert all(r.done >= r.arrival for r in served)
+    h.release()
+    ctx.close()
