@@ -48,8 +48,10 @@ N_VIEWS = 360
 METRIC = "projections/s at 256^3->512^2 (plain FP32)"
 WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
 # DRAM bytes (read + write) of one 360-view launch of the cell loop on this
-# workload, from one ncu capture (profiles/project_kernel_cells_256cubed_to_512sq_dram.md)
+# workload, from one ncu capture (profiles/project_kernel_cells_256cubed_to_512sq_dram.md),
+# with the launch shape it was captured at (views per block, lanes_x, rays per block, unroll)
 CELLS_TRAFFIC_BYTES = 7.90e9 + 0.75271e9
+CELLS_TRAFFIC_SHAPE = (2, 4, 256, 4)
 
 
 def make_inputs(n_views: int = N_VIEWS):
@@ -215,7 +217,9 @@ def run_ours(args):
                         storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage],
                         interp_mode=L.INTERP_TEXTURE if args.interp == "texture" else L.INTERP_SOFTWARE,
                         kernel={"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
-                                 "pairs": L.KERNEL_PAIRS}[args.kernel])
+                                 "pairs": L.KERNEL_PAIRS}[args.kernel],
+                        block_rays=args.block_rays, views_per_block=args.views_per_block, lanes_x=args.lanes_x,
+                        unroll=args.unroll)
     ctx = Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     vobj = VoxelVolume(vol, VOXEL)
@@ -226,7 +230,8 @@ def run_ours(args):
     samples = ctx.count_samples(volume, P, CHANNELS, ROWS, settings)
     tuned = None
     if settings.kernel == L.KERNEL_AUTO and settings.interp_mode == L.INTERP_SOFTWARE:
-        tuned = ctx.autotune(volume, P, CHANNELS, ROWS, settings)  # sample loop for this job
+        tuned = ctx.autotune(volume, P, CHANNELS, ROWS, settings)  # sample loop and launch shape for this job
+    ran = ctx.tuned_settings(volume, 1, CHANNELS, ROWS, settings)  # what the timed calls run
 
     def step():
         ctx.project(volume, dP, CHANNELS, ROWS, settings, out=out, stream=ctx.stream)
@@ -285,9 +290,11 @@ def run_ours(args):
         mhz = clk.get("sm_mhz") or 1965.0
         l1_peak = sms * 128 * mhz * 1e6 / 1e9  # GB/s
         achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-        loop = tuned[0] if tuned is not None else settings.kernel
+        loop = ran.kernel
+        shape = ran.launch_shape()
         traffic = (CELLS_TRAFFIC_BYTES if loop == L.KERNEL_CELLS and n_views == N_VIEWS and
-                   settings.storage == L.F32 and settings.interp_mode == L.INTERP_SOFTWARE else None)
+                   settings.storage == L.F32 and settings.interp_mode == L.INTERP_SOFTWARE and
+                   tuple(shape.values()) == CELLS_TRAFFIC_SHAPE else None)
         line = {
             "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -297,6 +304,9 @@ def run_ours(args):
             "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
             "config": {"workload": WORKLOAD, "views_per_step": n_views, "volume": "256^3", "detector": "512x512",
                        "interp": args.interp, "kernel": args.kernel,
+                       "loop": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs",
+                                L.KERNEL_GATHER: "gather"}.get(loop, "auto"),
+                       "launch_shape": shape,
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"views replicated per GPU x{world}"},
             "samples_per_step": samples,
@@ -757,7 +767,8 @@ def run_c5(args):
           {"workload": "8 resident 256^3 BF16 volumes; Poisson 2000/s; 1-16 perturbed views of 256^2 @1.2 mm",
            "budget_bytes": 40 * 10**9}, higher_is_better=False, serving_at_2000=at, capacity=cap,
           sweep=sweep, max_rate_p99_under_5ms=max(ok) if ok else None,
-          autotuned=[t[0] for t in getattr(server, "tuned", [])])
+          autotuned=[t[0] for t in getattr(server, "tuned", [])],
+          launch_shapes=[ctx.tuned_settings(v, 1, 256, 256, Settings(kernel=kernel)).launch_shape() for v in vols])
     for v in vols:
         v.release()
     ctx.close()
@@ -773,6 +784,11 @@ def main():
     ap.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32")
     ap.add_argument("--interp", choices=["software", "texture"], default="software")
     ap.add_argument("--kernel", choices=["auto", "gather", "cells", "pairs"], default="auto")
+    # launch shape (0 = autotuned with --kernel auto, else the library default)
+    ap.add_argument("--block-rays", type=int, default=0, choices=[0, 128, 256, 512])
+    ap.add_argument("--views-per-block", type=int, default=0, choices=[0, 1, 2, 4])
+    ap.add_argument("--lanes-x", type=int, default=0, choices=[0, 4, 8])
+    ap.add_argument("--unroll", type=int, default=0, choices=[0, 2, 4, 8])
     ap.add_argument("--views", type=int, default=N_VIEWS,
                     help="views per step (360 = the configuration; fewer = a small profiling case)")
     ap.add_argument("--e2e-steps", type=int, default=3)

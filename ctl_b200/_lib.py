@@ -10,6 +10,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libctlcu.so")
+ABI_VERSION = 2  # CTLCU_ABI_VERSION of include/ctlcu.h these bindings follow
 
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -46,7 +47,9 @@ class VolumeDesc(C.Structure):
 class Settings(C.Structure):
     _fields_ = [("rays_per_pixel", C.c_uint32 * 2), ("ray_sampling", C.c_float),
                 ("volume_upsampling", C.c_uint32), ("interpolate", C.c_int32),
-                ("interp_mode", C.c_int32), ("accum", C.c_int32), ("kernel", C.c_int32)]
+                ("interp_mode", C.c_int32), ("accum", C.c_int32), ("kernel", C.c_int32),
+                ("views_per_block", C.c_int32), ("lanes_x", C.c_int32), ("block_rays", C.c_int32),
+                ("unroll", C.c_int32)]
 
 
 TRAJ_HELICAL, TRAJ_AXIAL, TRAJ_WOBBLE, TRAJ_SHORT_SCAN, TRAJ_CIRCLE_PLUS_LINE = 0, 1, 2, 3, 4
@@ -107,6 +110,8 @@ SIGNATURES = [
     ("ctlcu_autotune", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                  C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_int),
                                  C.POINTER(C.c_float)]),
+    ("ctlcu_tuned_settings", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_uint32, C.c_uint32,
+                                       C.c_uint32, C.POINTER(Settings)]),
     ("ctlcu_view_setup", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                    C.c_void_p]),
     ("ctlcu_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -152,6 +157,9 @@ def load() -> C.CDLL:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
+        if lib.ctlcu_abi_version() != ABI_VERSION:
+            raise ImportError(f"{LIB_PATH} has ABI version {lib.ctlcu_abi_version()}, these bindings "
+                              f"expect {ABI_VERSION}; rebuild with `python -m ctl_b200.build`")
         _lib = lib
     return _lib
 

@@ -62,8 +62,12 @@ struct ctlcu_ctx {
     unsigned long long* d_counter = nullptr;
     uint64_t launches = 0;
     cudaEvent_t order = nullptr;  // orders caller streams after volume staging on `stream`
-    // autotuned sample-loop choice per (volume, channels, rows, modules)
-    std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, int> tuned;
+    // autotuned sample loop and launch shape per (volume, channels, rows, modules)
+    struct Tuned {
+        int kernel;
+        LaunchShape shape;
+    };
+    std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, Tuned> tuned;
     DenStaging den;  // pinned buffers for DEN file streaming, allocated on first use
     cudaStream_t copy_stream = nullptr;  // device-to-host copies that overlap projection
 };
@@ -130,7 +134,66 @@ int check_settings(ctlcu_ctx* ctx, const ctlcu_settings* s)
         (!s->interpolate || s->interp_mode != CTLCU_INTERP_SOFTWARE || s->volume_upsampling != 1))
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
                     "the cell kernel needs software trilinear interpolation and volumeUpSampling 1");
+    // launch shape: each field 0 (tuned or default) or one of its values
+    if (s->block_rays != 0 && s->block_rays != 128 && s->block_rays != 256 && s->block_rays != 512)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "block_rays must be 0, 128, 256 or 512 (got %d)", s->block_rays);
+    if (s->views_per_block != 0 && s->views_per_block != 1 && s->views_per_block != 2 && s->views_per_block != 4)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "views_per_block must be 0, 1, 2 or 4 (got %d)",
+                    s->views_per_block);
+    if (s->lanes_x != 0 && s->lanes_x != 4 && s->lanes_x != 8)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "lanes_x must be 0, 4 or 8 (got %d)", s->lanes_x);
+    if (s->unroll != 0 && s->unroll != 2 && s->unroll != 4 && s->unroll != 8)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unroll must be 0, 2, 4 or 8 (got %d)", s->unroll);
+    // with any of the three left 0, shape_of completes them to a valid shape
+    if (s->block_rays && s->views_per_block && s->lanes_x) {
+        LaunchShape sh;
+        sh.block = (uint32_t)s->block_rays;
+        sh.views = (uint32_t)s->views_per_block;
+        sh.lanes_x = (uint32_t)s->lanes_x;
+        if (const char* why = shape_error(sh))
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "launch shape %d rays / %d views / lanes_x %d: %s",
+                        s->block_rays, s->views_per_block, s->lanes_x, why);
+    }
     return CTLCU_OK;
+}
+
+// The launch shape of resolved settings: zero fields take the defaults (a
+// warp patch of 8x4 where 4x8 does not fit the tile).
+LaunchShape shape_of(const ctlcu_settings* s)
+{
+    LaunchShape sh;
+    if (s->block_rays)
+        sh.block = (uint32_t)s->block_rays;
+    if (s->views_per_block)
+        sh.views = (uint32_t)s->views_per_block;
+    if (s->unroll)
+        sh.unroll = (uint32_t)s->unroll;
+    if (s->lanes_x)
+        sh.lanes_x = (uint32_t)s->lanes_x;
+    else if (shape_error(sh))
+        sh.lanes_x = 8;
+    return sh;
+}
+
+// The shape fields of `s` filled in from `sh` where they are 0.
+void fill_shape(ctlcu_settings& s, const LaunchShape& sh)
+{
+    if (!s.block_rays)
+        s.block_rays = (int32_t)sh.block;
+    if (!s.views_per_block)
+        s.views_per_block = (int32_t)sh.views;
+    if (!s.lanes_x)
+        s.lanes_x = (int32_t)sh.lanes_x;
+    if (!s.unroll)
+        s.unroll = (int32_t)sh.unroll;
+}
+
+uint32_t log2u(uint32_t v)
+{
+    uint32_t r = 0;
+    while ((1u << r) < v)
+        ++r;
+    return r;
 }
 
 int check_desc(ctlcu_ctx* ctx, const ctlcu_volume_desc* d)
@@ -461,17 +524,27 @@ int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, Project
 
 void job_args(ProjectArgs& a, const ctlcu_settings* s, uint32_t V, uint32_t M, uint32_t C, uint32_t R)
 {
+    const LaunchShape sh = shape_of(s);
+    const uint32_t tx = shape_tile_x(sh.block, sh.views), ty = shape_tile_y(sh.block, sh.views);
     a.channels = C;
     a.rows = R;
     a.n_vm = V * M;
     a.n_modules = M;
-    a.tiles_x = (C + kTileX - 1) / kTileX;
-    a.tiles_per_vm = a.tiles_x * ((R + kTileY - 1) / kTileY);
+    a.tiles_x = (C + tx - 1) / tx;
+    a.tiles_per_vm = a.tiles_x * ((R + ty - 1) / ty);
     a.rays_x = s->rays_per_pixel[0];
     a.rays_y = s->rays_per_pixel[1];
     a.vm_group = CTLCU_VM_GROUP;
     a.n_views = V;
-    a.view_groups = (V + kViewsPerBlock - 1) / kViewsPerBlock;
+    a.view_groups = (V + sh.views - 1) / sh.views;
+    a.block = sh.block;
+    a.unroll = sh.unroll;
+    a.vpb_shift = log2u(sh.views);
+    a.wpv_shift = log2u(sh.block / 32 / sh.views);
+    a.lx_shift = log2u(sh.lanes_x);
+    a.wx_shift = log2u(tx / sh.lanes_x);
+    a.tx_shift = log2u(tx);
+    a.ty_shift = log2u(ty);
 }
 
 VolumeEntry* find_volume(ctlcu_ctx* ctx, uint64_t h)
@@ -493,19 +566,29 @@ int order_after_staging(ctlcu_ctx* ctx, cudaStream_t st)
 
 // Setup + projection on `s` with device pmats/out.  Scratch comes from the
 // stream-ordered pool, so concurrent calls on different streams do not share it.
-// CTLCU_KERNEL_AUTO resolved: the autotuned choice for this volume and
-// detector if there is one, else the cell kernel where it applies.
+// CTLCU_KERNEL_AUTO resolved: the autotuned loop for this volume and detector
+// if there is one, else the cell loop where it applies.  Launch-shape fields
+// left 0 take the tuned shape when the loop is the tuned one, else the
+// defaults, so every shape field of the result is set.
 ctlcu_settings resolve_kernel(ctlcu_ctx* ctx, const VolumeEntry& v, const ctlcu_settings* s, uint32_t C, uint32_t R,
                               uint32_t M)
 {
     ctlcu_settings e = *s;
-    if (e.kernel != CTLCU_KERNEL_AUTO)
-        return e;
     const bool fast = e.interpolate && e.interp_mode == CTLCU_INTERP_SOFTWARE && e.volume_upsampling == 1;
-    if (!fast)
-        return e;
     auto it = ctx->tuned.find(std::make_tuple(v.handle, C, R, M));
-    e.kernel = it != ctx->tuned.end() ? it->second : CTLCU_KERNEL_CELLS;
+    const bool have = it != ctx->tuned.end();
+    if (e.kernel == CTLCU_KERNEL_AUTO && fast)
+        e.kernel = have ? it->second.kernel : CTLCU_KERNEL_CELLS;
+    const int loop = e.kernel == CTLCU_KERNEL_AUTO ? CTLCU_KERNEL_GATHER : e.kernel;
+    if (have && fast && loop == it->second.kernel) {
+        ctlcu_settings t = e;
+        fill_shape(t, it->second.shape);
+        if (!shape_error(shape_of(&t))) {
+            fill_shape(e, it->second.shape);
+            return e;
+        }
+    }
+    fill_shape(e, shape_of(&e));
     return e;
 }
 
@@ -632,6 +715,7 @@ struct BatchPrep {
     uint32_t total_vm = 0, total_items = 0;
     Accum acc = Accum::F64;
     Mode mode = Mode::Cells;        // Cells or Pairs, the same for every request
+    LaunchShape shape;              // the same for every request
 };
 
 struct BatchDevice {
@@ -662,9 +746,11 @@ int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, con
     if (!bp.persistent)
         return CTLCU_OK;
     bp.acc = (Accum)s->accum;
-    // one sample loop for the whole launch: the first request's (autotuned) choice
+    // one sample loop and launch shape for the whole launch: the first request's
+    // (autotuned) choice
     const ctlcu_settings eff = resolve_kernel(ctx, *find_volume(ctx, requests[0].volume), s, requests[0].channels,
                                               requests[0].rows, requests[0].n_modules);
+    bp.shape = shape_of(&eff);
     uint64_t vm = 0, items = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const ctlcu_request& q = requests[i];
@@ -677,7 +763,7 @@ int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, con
         if (mode != Mode::Cells && mode != Mode::Pairs)
             return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u does not take the cell kernel", i);
         bp.mode = mode;
-        job_args(br.a, s, q.n_views, q.n_modules, q.channels, q.rows);
+        job_args(br.a, &eff, q.n_views, q.n_modules, q.channels, q.rows);
         br.a.out = q.out;
         br.a.flags = ctx->d_flags;
         br.a.counter = nullptr;
@@ -720,7 +806,7 @@ int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, co
     CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int), st));
     CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
     int blocks = 0;
-    CU_TRY(ctx, launch_batch(bd.reqs, n, bp.total_items, bp.mode, bp.acc, bd.counter, &blocks, st));
+    CU_TRY(ctx, launch_batch(bd.reqs, n, bp.total_items, bp.mode, bp.acc, bp.shape, bd.counter, &blocks, st));
     ctx->launches += 2;
     return CTLCU_OK;
 }
@@ -859,6 +945,7 @@ ctlcu_settings ctlcu_settings_default(void)
     s.interp_mode = CTLCU_INTERP_SOFTWARE;
     s.accum = CTLCU_ACCUM_FP64;
     s.kernel = CTLCU_KERNEL_AUTO;
+    s.views_per_block = s.lanes_x = s.block_rays = s.unroll = 0;  // tuned or default launch shape
     return s;
 }
 
@@ -1355,32 +1442,74 @@ int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settin
         cleanup();
         return fail(ctx, CTLCU_ERR_OUT_OF_MEMORY, "autotune scratch allocation failed");
     }
+    // mean time of 3 runs after one that builds the loop's array and warms the caches
+    auto time_runs = [&](const ctlcu_settings& t, float& out_ms) {
+        int rr = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
+        if (rr)
+            return rr;
+        cudaEventRecord(e0, ctx->stream);
+        for (int k = 0; k < 3 && rr == CTLCU_OK; ++k)
+            rr = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (rr)
+            return rr;
+        if (cudaEventSynchronize(e1) != cudaSuccess)
+            return fail(ctx, CTLCU_ERR_CUDA, "autotune run failed");
+        cudaEventElapsedTime(&out_ms, e0, e1);
+        out_ms /= 3.0f;
+        return (int)CTLCU_OK;
+    };
+    // 1. the sample loop, with the caller's launch shape (defaults where 0)
     for (int c = 0; c < 3 && r == CTLCU_OK; ++c) {
         ctlcu_settings t = s;
         t.kernel = cand[c];
-        // first run builds the variant's array and warms the caches
-        r = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
-        if (r)
-            break;
-        cudaEventRecord(e0, ctx->stream);
-        for (int k = 0; k < 3 && r == CTLCU_OK; ++k)
-            r = project_device(ctx, *v, &t, d_pm, nv, n_modules, channels, rows, d_out, ctx->stream);
-        cudaEventRecord(e1, ctx->stream);
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            r = fail(ctx, CTLCU_ERR_CUDA, "autotune run failed");
-            break;
-        }
-        cudaEventElapsedTime(&ms[c], e0, e1);
-        ms[c] /= 3.0f;
+        fill_shape(t, shape_of(&t));
+        r = time_runs(t, ms[c]);
     }
-    cleanup();
-    if (r)
-        return r;
     int best = 0;
     for (int c = 1; c < 3; ++c)
         if (ms[c] < ms[best])
             best = c;
-    ctx->tuned[std::make_tuple(volume, channels, rows, n_modules)] = cand[best];
+    // 2. the launch shape of that loop, one field at a time; a change is kept
+    // when it is at least 1% faster, so timing noise does not flip a choice
+    ctlcu_settings bs = s;
+    bs.kernel = cand[best];
+    fill_shape(bs, shape_of(&bs));
+    float best_ms = ms[best];
+    struct Field {
+        int32_t ctlcu_settings::*f;
+        int32_t caller;
+        int32_t values[3];
+    };
+    const Field fields[4] = { { &ctlcu_settings::views_per_block, s.views_per_block, { 1, 2, 4 } },
+                              { &ctlcu_settings::lanes_x, s.lanes_x, { 4, 8, 0 } },
+                              { &ctlcu_settings::block_rays, s.block_rays, { 128, 256, 512 } },
+                              { &ctlcu_settings::unroll, s.unroll, { 2, 4, 8 } } };
+    for (const Field& fd : fields) {
+        if (fd.caller != 0 || r != CTLCU_OK)
+            continue;  // fixed by the caller
+        if (fd.f == &ctlcu_settings::unroll && bs.kernel == CTLCU_KERNEL_GATHER)
+            continue;  // the gather loop has no partial sums
+        const int32_t current = bs.*(fd.f);
+        for (int32_t value : fd.values) {
+            if (value == 0 || value == current || r != CTLCU_OK)
+                continue;
+            ctlcu_settings t = bs;
+            t.*(fd.f) = value;
+            if (shape_error(shape_of(&t)))
+                continue;
+            float m = 0.f;
+            r = time_runs(t, m);
+            if (r == CTLCU_OK && m < 0.99f * best_ms) {
+                best_ms = m;
+                bs = t;
+            }
+        }
+    }
+    cleanup();
+    if (r)
+        return r;
+    ctx->tuned[std::make_tuple(volume, channels, rows, n_modules)] = ctlcu_ctx::Tuned{ cand[best], shape_of(&bs) };
     // keep only the array the chosen loop reads
     cudaStreamSynchronize(ctx->stream);
     if (cand[best] != CTLCU_KERNEL_CELLS && v->cells) {
@@ -1400,6 +1529,27 @@ int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settin
         for (int c = 0; c < 3; ++c)
             ms_out[c] = ms[c];
     return read_flags(ctx);
+}
+
+int ctlcu_tuned_settings(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings, uint32_t n_modules,
+                         uint32_t channels, uint32_t rows, ctlcu_settings* out)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!out)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "out is NULL");
+    int r = check_settings(ctx, settings);
+    if (r)
+        return r;
+    r = check_job(ctx, 1, n_modules, channels, rows);
+    if (r)
+        return r;
+    VolumeEntry* v = find_volume(ctx, volume);
+    if (!v)
+        return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
+    *out = resolve_kernel(ctx, *v, settings, channels, rows, n_modules);
+    return CTLCU_OK;
 }
 
 int ctlcu_view_setup(ctlcu_ctx* ctx, const double* pmats, uint32_t n_views, uint32_t n_modules,

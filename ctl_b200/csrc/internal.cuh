@@ -17,44 +17,60 @@ namespace ctlcu {
 // OpenCL CLK_ADDRESS_CLAMP border of the reference (border colour 0).
 constexpr int kPad = 2;
 
-// Compile-time tuning of the sample loops (defaults are the measured best).
-#ifndef CTLCU_VIEWS_PER_BLOCK
-#define CTLCU_VIEWS_PER_BLOCK 2  // views sharing one thread block (1, 2 or 4)
+// Register budgets of the sample loops (measured best; see the launch shapes below).
+#ifndef CTLCU_CELL_MAXREG
+#define CTLCU_CELL_MAXREG 48  // cell and pair loops: 5 blocks of 256 threads per SM
 #endif
-#ifndef CTLCU_CELL_MINB
-#define CTLCU_CELL_MINB 5  // resident blocks per SM the register budget is sized for
-#endif
-#ifndef CTLCU_CELL_UNROLL
-#define CTLCU_CELL_UNROLL 4  // samples per partial sum
-#endif
-#ifndef CTLCU_LANES_X
-#define CTLCU_LANES_X 4  // lanes of a warp along the channels (8: 8x4 patch, 4: 4x8, 16: 16x2)
+#ifndef CTLCU_GATHER_MAXREG
+#define CTLCU_GATHER_MAXREG 80  // gather, nearest-voxel and texture loops: 3 blocks of 256 per SM
 #endif
 #ifndef CTLCU_VM_GROUP
 #define CTLCU_VM_GROUP 8  // view groups per chunk in the block order
 #endif
 
-// A thread block holds 256 rays: one detector tile of kTileX x kTileY pixels
-// for each of kViewsPerBlock consecutive views of one module.  Adjacent views
-// of a scan see a tile through nearly the same part of the volume, so their
-// rays share cached cells.  Each warp is a kLanesX x kLanesY pixel patch of
-// one view, so its 32 rays are neighbours.
-#ifndef CTLCU_BLOCK
-#define CTLCU_BLOCK 256  // threads per block (256, 512 or 1024)
-#endif
-constexpr int kBlock = CTLCU_BLOCK;
-constexpr int kViewsPerBlock = CTLCU_VIEWS_PER_BLOCK;
-constexpr int kTileX = (kViewsPerBlock <= 2 || kBlock >= 512) ? 16 : 8;
-constexpr int kTileY = kBlock / (kTileX * kViewsPerBlock);
-constexpr int kWarpsPerView = kBlock / 32 / kViewsPerBlock;
-constexpr int kLanesX = CTLCU_LANES_X;
-constexpr int kLanesY = 32 / kLanesX;
-constexpr int kWarpsX = kTileX / kLanesX;
-static_assert(kViewsPerBlock >= 1 && kViewsPerBlock <= 8 && (kViewsPerBlock & (kViewsPerBlock - 1)) == 0,
-              "views per block");
-static_assert(kBlock == 256 || kBlock == 512 || kBlock == 1024, "block size");
-static_assert(kTileX % kLanesX == 0 && kTileY % kLanesY == 0, "lane patch must tile the block tile");
-static_assert(kWarpsX * (kTileY / kLanesY) == kWarpsPerView, "warps must cover the tile exactly");
+// Launch shape of the projection kernels, chosen per call at run time
+// (ctlcu_settings views_per_block, lanes_x, block_rays, unroll; the
+// autotuner picks them per volume and detector).  A thread block holds
+// `block` rays: one detector tile of tile_x x tile_y pixels for each of
+// `views` consecutive views of one module.  Adjacent views of a scan see a
+// tile through nearly the same part of the volume, so their rays share cached
+// cells.  Each warp is a lanes_x x (32 / lanes_x) pixel patch of one view, so
+// its 32 rays are neighbours.  `unroll` samples of the cell and pair loops
+// form one FP32 partial sum before it goes to the accumulator.
+struct LaunchShape {
+    uint32_t block = 256;   // rays (threads) per block: 128, 256 or 512
+    uint32_t views = 2;     // views per block: 1, 2 or 4
+    uint32_t lanes_x = 4;   // lanes of a warp along the channels: 4 (4x8 patch) or 8 (8x4)
+    uint32_t unroll = 4;    // samples per partial sum: 2, 4 or 8
+};
+constexpr uint32_t kMaxBlock = 512;
+
+// Tile of a shape: pixels per view = block / views, 16 channels wide from 128
+// pixels up, else 8.
+__host__ __device__ constexpr uint32_t shape_tile_x(uint32_t block, uint32_t views)
+{
+    return block / views >= 128 ? 16u : 8u;
+}
+__host__ __device__ constexpr uint32_t shape_tile_y(uint32_t block, uint32_t views)
+{
+    return block / views / shape_tile_x(block, views);
+}
+
+// Null if the shape is valid, else what is wrong with it.
+inline const char* shape_error(const LaunchShape& s)
+{
+    if (s.block != 128 && s.block != 256 && s.block != 512)
+        return "block_rays must be 128, 256 or 512";
+    if (s.views != 1 && s.views != 2 && s.views != 4)
+        return "views_per_block must be 1, 2 or 4";
+    if (s.lanes_x != 4 && s.lanes_x != 8)
+        return "lanes_x must be 4 or 8";
+    if (s.unroll != 2 && s.unroll != 4 && s.unroll != 8)
+        return "unroll must be 2, 4 or 8";
+    if (shape_tile_y(s.block, s.views) % (32u / s.lanes_x) != 0)
+        return "the warp patch (lanes_x x 32/lanes_x) does not tile the detector tile of this block";
+    return nullptr;
+}
 
 // Error bits raised by kernels into the context's device flag word.
 constexpr int kFlagSingular = 1;   // a projection matrix with singular / non-finite M
@@ -128,12 +144,6 @@ __host__ __device__ __forceinline__ uint32_t cell_linear(uint32_t ix, uint32_t i
 #define CTLCU_CELL_CACHE 2  // 0: load every sample; 1: load on cell change (branch); 2: predicated load;
                             // 3: texture fetch on change
 #endif
-#ifndef CTLCU_CELL_RAYS
-#define CTLCU_CELL_RAYS 1  // rays per thread in the cell kernel (1 or 2)
-#endif
-#ifndef CTLCU_CELL2_MINB
-#define CTLCU_CELL2_MINB 8  // resident 128-thread blocks per SM for two rays per thread
-#endif
 
 #ifndef CTLCU_CELL_PREFETCH
 #define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
@@ -187,7 +197,15 @@ struct ProjectArgs {
     uint32_t cmax;            // last valid cell index
     uint32_t vm_group;        // view groups per chunk of the block order
     uint32_t n_views;         // views (n_vm / n_modules)
-    uint32_t view_groups;     // ceil(n_views / kViewsPerBlock)
+    uint32_t view_groups;     // ceil(n_views / views per block)
+    // launch shape (LaunchShape), as block size and log2 factors of the pixel mapping
+    uint32_t block;           // threads per block
+    uint32_t unroll;          // samples per partial sum (cell and pair loops)
+    uint32_t vpb_shift;       // log2 views per block
+    uint32_t wpv_shift;       // log2 warps per view
+    uint32_t lx_shift;        // log2 lanes along the channels
+    uint32_t wx_shift;        // log2 warps along the channels of a tile
+    uint32_t tx_shift, ty_shift;  // log2 tile width and height
     const ViewGeom* geom;     // [n_vm]
     float* out;               // [n_vm][rows][channels]
     uint32_t channels, rows;
@@ -218,9 +236,10 @@ struct BatchReq {
 cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t total, ViewGeom* geom,
                                int* flags, cudaStream_t s);
 // Persistent launch (Mode::Cells or Mode::Pairs) over all work items of a
-// batch; `counter` must be zero at launch.  Returns the grid size in *blocks.
+// batch, every request with the launch shape `shape` (block size and unroll);
+// `counter` must be zero at launch.  Returns the grid size in *blocks.
 cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
-                         unsigned int* counter, int* blocks, cudaStream_t s);
+                         const LaunchShape& shape, unsigned int* counter, int* blocks, cudaStream_t s);
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,
                          double* qr_out, double* src_out, int* flags, cudaStream_t s);
 cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype, cudaStream_t s);

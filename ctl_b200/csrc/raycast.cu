@@ -1,7 +1,8 @@
 // Cone-beam ray casting kernels (sm_100a).
 //
-// One thread per detector pixel; a block covers a 16x16 detector tile of one
-// (view, module), each warp an 8x4 patch.  Per ray, in FP64: direction
+// One thread per detector pixel; a block covers one detector tile of a few
+// neighbouring views of one module, each warp a small pixel patch of one view
+// (LaunchShape, chosen per call).  Per ray, in FP64: direction
 // A*[x,y,1] normalised and scaled to one step in voxel units, entry/exit
 // parameters against the (half-voxel padded) volume box with the 0.01-voxel
 // face tolerance, first/last sample index.  The sample loop then runs in FP32
@@ -351,9 +352,9 @@ __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const cha
     return fmaf(hz, g.y, g.x);
 }
 
-// Sample loop over the coefficient cells, CTLCU_CELL_UNROLL samples per
-// partial sum (FP32) handed to the accumulator.
-template <Accum ACC>
+// Sample loop over the coefficient cells, U samples per partial sum (FP32)
+// handed to the accumulator.
+template <Accum ACC, int U>
 __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
     const char* __restrict__ cells = static_cast<const char*>(a.cells);
@@ -366,11 +367,11 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
     float2 kk = make_float2(0.0f, 0.0f);
     CellCache cc;
 #if CTLCU_CELL_PREFETCH > 0
-    __shared__ float prefetch_sink[kBlock];
+    __shared__ float prefetch_sink[kMaxBlock];
     const uint32_t prefetch_slot = (uint32_t)__cvta_generic_to_shared(&prefetch_sink[threadIdx.x]);
 #endif
     int k = 0;
-    for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
+    for (; k + U <= r.n; k += U) {
         float part = 0.0f;
 #if CTLCU_CELL_PREFETCH > 0
         {
@@ -383,14 +384,14 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
         }
 #endif
 #pragma unroll
-        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
-            part += cell_sample(a.cell_tex, cells,kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
+        for (int j = 0; j < U; ++j) {
+            part += cell_sample(a.cell_tex, cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
             kk = __fadd2_rn(kk, one2);
         }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(cell_sample(a.cell_tex, cells,kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
+        acc.add(cell_sample(a.cell_tex, cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
         kk = __fadd2_rn(kk, one2);
     }
 #if CTLCU_CELL_PREFETCH > 0
@@ -448,7 +449,7 @@ __device__ __forceinline__ float pair_sample(const char* __restrict__ pairs, flo
 }
 
 // Sample loop over the x-pair array (same structure as march_cells).
-template <Accum ACC>
+template <Accum ACC, int U>
 __device__ __forceinline__ void march_pairs(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
     const char* __restrict__ pairs = static_cast<const char*>(a.cells);
@@ -461,10 +462,10 @@ __device__ __forceinline__ void march_pairs(const ProjectArgs& a, const Ray& r, 
     float2 kk = make_float2(0.0f, 0.0f);
     PairCache pc;
     int k = 0;
-    for (; k + CTLCU_CELL_UNROLL <= r.n; k += CTLCU_CELL_UNROLL) {
+    for (; k + U <= r.n; k += U) {
         float part = 0.0f;
 #pragma unroll
-        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
+        for (int j = 0; j < U; ++j) {
             part += pair_sample(pairs, kk, bxy, bz, dxy, dz, sy, sz, pmax, pc);
             kk = __fadd2_rn(kk, one2);
         }
@@ -488,7 +489,8 @@ __device__ __forceinline__ void march_texture(const ProjectArgs& a, const Ray& r
     }
 }
 
-// Pixel of thread `tid` of work item (block) `b` of kBlock threads.
+// Pixel of thread `tid` of work item (block) `b` of a.block threads, for the
+// launch shape in `a` (every factor of the mapping is a power of two).
 __device__ __forceinline__ bool pixel_of_item(const ProjectArgs& a, uint32_t b, uint32_t tid, uint32_t& vm,
                                               uint32_t& x, uint32_t& y)
 {
@@ -508,12 +510,13 @@ __device__ __forceinline__ bool pixel_of_item(const ProjectArgs& a, uint32_t b, 
     const uint32_t m = q / T;
     const uint32_t t = q - m * T;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
-    const uint32_t slot = warp / kWarpsPerView, w = warp - slot * kWarpsPerView;
-    const uint32_t view = vg * kViewsPerBlock + slot;
+    const uint32_t slot = warp >> a.wpv_shift, w = warp & ((1u << a.wpv_shift) - 1u);
+    const uint32_t view = (vg << a.vpb_shift) + slot;
     vm = view * a.n_modules + m;
     const uint32_t ty = t / a.tiles_x, tx = t - ty * a.tiles_x;
-    x = tx * kTileX + (w % kWarpsX) * kLanesX + (lane % kLanesX);
-    y = ty * kTileY + (w / kWarpsX) * kLanesY + (lane / kLanesX);
+    const uint32_t ly_shift = 5u - a.lx_shift;
+    x = (tx << a.tx_shift) + ((w & ((1u << a.wx_shift) - 1u)) << a.lx_shift) + (lane & ((1u << a.lx_shift) - 1u));
+    y = (ty << a.ty_shift) + ((w >> a.wx_shift) << ly_shift) + (lane >> a.lx_shift);
     return view < a.n_views && x < a.channels && y < a.rows;
 }
 
@@ -528,8 +531,8 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
     return pixel_of_thread(a, threadIdx.x, vm, x, y);
 }
 
-// The rays of work item `b` for thread `tid`, cell kernel (FP32 cells).
-template <Mode M, Accum ACC>
+// The rays of work item `b` for thread `tid`, cell or pair loop (FP32 entries).
+template <Mode M, Accum ACC, int U>
 __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uint32_t tid)
 {
     uint32_t vm, x, y;
@@ -549,19 +552,26 @@ __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uin
             const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
             const Ray r = setup_ray<M>(a, g, px, py, a.flags);
             if (M == Mode::Pairs)
-                march_pairs<ACC>(a, r, acc);
+                march_pairs<ACC, U>(a, r, acc);
             else
-                march_cells<ACC>(a, r, acc);
+                march_cells<ACC, U>(a, r, acc);
         }
     *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
+}
+
+// Cell or pair loop over one block of the regular grid.
+template <Mode M, Accum ACC, int U>
+__global__ void __maxnreg__(CTLCU_CELL_MAXREG) cells_kernel(const ProjectArgs a)
+{
+    cells_item<M, ACC, U>(a, blockIdx.x, threadIdx.x);
 }
 
 // Persistent batch kernel: blocks take work items in order from `counter`
 // until all requests' items are done.  Work items of one request are its
 // blocks in the order of the single-request launch, so blocks running at the
 // same time work on neighbouring views of one volume.
-template <Mode M, Accum ACC>
-__global__ void __launch_bounds__(kBlock, CTLCU_CELL_MINB)
+template <Mode M, Accum ACC, int U>
+__global__ void __maxnreg__(CTLCU_CELL_MAXREG)
     batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter)
 {
     __shared__ ProjectArgs sa;
@@ -593,94 +603,16 @@ __global__ void __launch_bounds__(kBlock, CTLCU_CELL_MINB)
         for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
             dst[i] = src[i];
         __syncthreads();
-        cells_item<M, ACC>(sa, s_local, threadIdx.x);
+        cells_item<M, ACC, U>(sa, s_local, threadIdx.x);
         __syncthreads();
     }
 }
 
-// Two rays per thread: the cell loops of both run interleaved, so each warp
-// keeps two independent load chains in flight.  A block of kBlock/2 threads
-// covers the same pixels as a kBlock-thread block; thread t takes the pixels
-// of threads t and t + kBlock/2 of that layout (the same pixel of two
-// neighbouring views when kViewsPerBlock is 2).
-template <Accum ACC>
-__device__ __forceinline__ void march_cells2(const ProjectArgs& a, const Ray& r0, const Ray& r1,
-                                             Accumulator<ACC>& acc0, Accumulator<ACC>& acc1)
-{
-    const char* __restrict__ cells = static_cast<const char*>(a.cells);
-    const float2 b0 = make_float2((float)r0.base[0], (float)r0.base[1]);
-    const float b0z = (float)r0.base[2];
-    const float2 d0 = make_float2((float)r0.step[0], (float)r0.step[1]);
-    const float d0z = (float)r0.step[2];
-    const float2 b1 = make_float2((float)r1.base[0], (float)r1.base[1]);
-    const float b1z = (float)r1.base[2];
-    const float2 d1 = make_float2((float)r1.step[0], (float)r1.step[1]);
-    const float d1z = (float)r1.step[2];
-    const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
-    const float2 one2 = make_float2(1.0f, 1.0f);
-    float2 kk = make_float2(0.0f, 0.0f);
-    CellCache c0, c1;
-    const int nc = min(r0.n, r1.n);
-    int k = 0;
-    for (; k + CTLCU_CELL_UNROLL <= nc; k += CTLCU_CELL_UNROLL) {
-        float p0 = 0.0f, p1 = 0.0f;
-#pragma unroll
-        for (int j = 0; j < CTLCU_CELL_UNROLL; ++j) {
-            p0 += cell_sample(a.cell_tex, cells,kk, b0, b0z, d0, d0z, sy, sz, cmax, c0);
-            p1 += cell_sample(a.cell_tex, cells,kk, b1, b1z, d1, d1z, sy, sz, cmax, c1);
-            kk = __fadd2_rn(kk, one2);
-        }
-        acc0.add(p0);
-        acc1.add(p1);
-    }
-    float2 kk0 = kk;
-    for (int k0 = k; k0 < r0.n; ++k0) {
-        acc0.add(cell_sample(a.cell_tex, cells,kk0, b0, b0z, d0, d0z, sy, sz, cmax, c0));
-        kk0 = __fadd2_rn(kk0, one2);
-    }
-    for (int k1 = k; k1 < r1.n; ++k1) {
-        acc1.add(cell_sample(a.cell_tex, cells,kk, b1, b1z, d1, d1z, sy, sz, cmax, c1));
-        kk = __fadd2_rn(kk, one2);
-    }
-}
-
-template <Accum ACC>
-__global__ void __launch_bounds__(kBlock / 2, CTLCU_CELL2_MINB) project_cells2_kernel(const ProjectArgs a)
-{
-    uint32_t vm0, x0, y0, vm1, x1, y1;
-    const bool ok0 = pixel_of_thread(a, threadIdx.x, vm0, x0, y0);
-    const bool ok1 = pixel_of_thread(a, threadIdx.x + kBlock / 2, vm1, x1, y1);
-    if (!ok0 && !ok1)
-        return;
-    const ViewGeom& g0 = a.geom[ok0 ? vm0 : vm1];
-    const ViewGeom& g1 = a.geom[ok1 ? vm1 : vm0];
-    const bool run0 = ok0 && g0.valid, run1 = ok1 && g1.valid;
-    Accumulator<ACC> acc0, acc1;
-    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
-    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
-        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
-            const double ox = -0.5 + 0.5 * ix + rx * ix, oy = -0.5 + 0.5 * iy + ry * iy;
-            Ray r0 = setup_ray<Mode::Cells>(a, g0, (double)x0 + ox, (double)y0 + oy, a.flags);
-            Ray r1 = setup_ray<Mode::Cells>(a, g1, (double)x1 + ox, (double)y1 + oy, a.flags);
-            if (!run0)
-                r0.n = 0;
-            if (!run1)
-                r1.n = 0;
-            march_cells2<ACC>(a, r0, r1, acc0, acc1);
-        }
-    const double nrays = (double)(a.rays_x * a.rays_y);
-    if (ok0)
-        a.out[((size_t)vm0 * a.rows + y0) * a.channels + x0] =
-            run0 ? (float)(a.increment * acc0.value() / nrays) : 0.0f;
-    if (ok1)
-        a.out[((size_t)vm1 * a.rows + y1) * a.channels + x1] =
-            run1 ? (float)(a.increment * acc1.value() / nrays) : 0.0f;
-}
-
+// Gather, nearest-voxel and texture loops over one block of the regular grid.
 template <typename T, Mode M, Accum ACC, bool UP>
-__global__ void __launch_bounds__(kBlock, (M == Mode::Cells || M == Mode::Pairs) ? CTLCU_CELL_MINB : 3)
-    project_kernel(const ProjectArgs a)
+__global__ void __maxnreg__(CTLCU_GATHER_MAXREG) project_kernel(const ProjectArgs a)
 {
+    static_assert(M == Mode::Trilinear || M == Mode::Nearest || M == Mode::Texture, "cells_kernel runs these");
     uint32_t vm, x, y;
     if (!pixel_of(a, vm, x, y))
         return;
@@ -697,11 +629,7 @@ __global__ void __launch_bounds__(kBlock, (M == Mode::Cells || M == Mode::Pairs)
             const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
             const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
             const Ray r = setup_ray<M>(a, g, px, py, a.flags);
-            if (M == Mode::Cells)
-                march_cells<ACC>(a, r, acc);
-            else if (M == Mode::Pairs)
-                march_pairs<ACC>(a, r, acc);
-            else if (M == Mode::Trilinear)
+            if (M == Mode::Trilinear)
                 march_trilinear<T, ACC, UP>(a, r, acc);
             else if (M == Mode::Nearest)
                 march_nearest<T, ACC>(a, r, acc);
@@ -712,7 +640,7 @@ __global__ void __launch_bounds__(kBlock, (M == Mode::Cells || M == Mode::Pairs)
 }
 
 template <Mode M>
-__global__ void __launch_bounds__(kBlock) count_kernel(const ProjectArgs a)
+__global__ void __launch_bounds__(kMaxBlock) count_kernel(const ProjectArgs a)
 {
     uint32_t vm, x, y;
     unsigned long long n = 0;
@@ -734,43 +662,49 @@ __global__ void __launch_bounds__(kBlock) count_kernel(const ProjectArgs a)
         atomicAdd(a.counter, n);
 }
 
+// The launch's block size must be one the pixel mapping was built for.
+bool block_ok(const ProjectArgs& a)
+{
+    return a.block == 128 || a.block == 256 || a.block == kMaxBlock;
+}
+
 template <Mode M, Accum ACC, bool UP>
 cudaError_t launch_typed(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
 {
     switch (dtype) {
-    case 0: project_kernel<float, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
-    case 1: project_kernel<__nv_bfloat16, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
-    case 2: project_kernel<__half, M, ACC, UP><<<grid, kBlock, 0, s>>>(a); break;
+    case 0: project_kernel<float, M, ACC, UP><<<grid, a.block, 0, s>>>(a); break;
+    case 1: project_kernel<__nv_bfloat16, M, ACC, UP><<<grid, a.block, 0, s>>>(a); break;
+    case 2: project_kernel<__half, M, ACC, UP><<<grid, a.block, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
 template <Mode M, Accum ACC>
-cudaError_t launch_mode(const ProjectArgs& a, int dtype, dim3 grid, cudaStream_t s)
+cudaError_t launch_cells(const ProjectArgs& a, dim3 grid, cudaStream_t s)
 {
-    if (M == Mode::Cells && CTLCU_CELL_RAYS == 2) {
-        project_cells2_kernel<ACC><<<grid, kBlock / 2, 0, s>>>(a);
-        return cudaGetLastError();
+    switch (a.unroll) {
+    case 2: cells_kernel<M, ACC, 2><<<grid, a.block, 0, s>>>(a); break;
+    case 4: cells_kernel<M, ACC, 4><<<grid, a.block, 0, s>>>(a); break;
+    case 8: cells_kernel<M, ACC, 8><<<grid, a.block, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
     }
-    if (M == Mode::Texture || M == Mode::Cells || M == Mode::Pairs) {
-        project_kernel<float, M, ACC, false><<<grid, kBlock, 0, s>>>(a);
-        return cudaGetLastError();
-    }
-    if (M == Mode::Trilinear && a.up != 1)
-        return launch_typed<M, ACC, true>(a, dtype, grid, s);
-    return launch_typed<M, ACC, false>(a, dtype, grid, s);
+    return cudaGetLastError();
 }
 
 template <Accum ACC>
 cudaError_t launch_acc(const ProjectArgs& a, Mode mode, int dtype, dim3 grid, cudaStream_t s)
 {
     switch (mode) {
-    case Mode::Trilinear: return launch_mode<Mode::Trilinear, ACC>(a, dtype, grid, s);
-    case Mode::Nearest: return launch_mode<Mode::Nearest, ACC>(a, dtype, grid, s);
-    case Mode::Texture: return launch_mode<Mode::Texture, ACC>(a, dtype, grid, s);
-    case Mode::Cells: return launch_mode<Mode::Cells, ACC>(a, dtype, grid, s);
-    case Mode::Pairs: return launch_mode<Mode::Pairs, ACC>(a, dtype, grid, s);
+    case Mode::Trilinear:
+        return a.up != 1 ? launch_typed<Mode::Trilinear, ACC, true>(a, dtype, grid, s)
+                         : launch_typed<Mode::Trilinear, ACC, false>(a, dtype, grid, s);
+    case Mode::Nearest: return launch_typed<Mode::Nearest, ACC, false>(a, dtype, grid, s);
+    case Mode::Texture:
+        project_kernel<float, Mode::Texture, ACC, false><<<grid, a.block, 0, s>>>(a);
+        return cudaGetLastError();
+    case Mode::Cells: return launch_cells<Mode::Cells, ACC>(a, grid, s);
+    case Mode::Pairs: return launch_cells<Mode::Pairs, ACC>(a, grid, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -782,7 +716,7 @@ cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype
     const uint64_t blocks = (uint64_t)a.view_groups * a.n_modules * a.tiles_per_vm;
     if (blocks == 0)
         return cudaSuccess;
-    if (blocks > 0x7fffffffull)
+    if (blocks > 0x7fffffffull || !block_ok(a))
         return cudaErrorInvalidConfiguration;
     const dim3 grid((unsigned)blocks);
     switch (acc) {
@@ -794,48 +728,62 @@ cudaError_t launch_project(const ProjectArgs& a, Mode mode, Accum acc, int dtype
 }
 
 namespace {
-template <Mode M, Accum ACC>
-cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter,
-                               int* blocks, cudaStream_t s)
+template <Mode M, Accum ACC, int U>
+cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, uint32_t block,
+                               unsigned int* counter, int* blocks, cudaStream_t s)
 {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<M, ACC>, kBlock, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<M, ACC, U>, (int)block, 0);
     if (e != cudaSuccess)
         return e;
     uint64_t grid = (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
     if (grid > total)
         grid = total;
     *blocks = (int)grid;
-    batch_cells_kernel<M, ACC><<<(unsigned)grid, kBlock, 0, s>>>(reqs, n_reqs, total, counter);
+    batch_cells_kernel<M, ACC, U><<<(unsigned)grid, block, 0, s>>>(reqs, n_reqs, total, counter);
     return cudaGetLastError();
+}
+
+template <Mode M, Accum ACC>
+cudaError_t launch_batch_unroll(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, const LaunchShape& sh,
+                                unsigned int* counter, int* blocks, cudaStream_t s)
+{
+    switch (sh.unroll) {
+    case 2: return launch_batch_typed<M, ACC, 2>(reqs, n_reqs, total, sh.block, counter, blocks, s);
+    case 4: return launch_batch_typed<M, ACC, 4>(reqs, n_reqs, total, sh.block, counter, blocks, s);
+    case 8: return launch_batch_typed<M, ACC, 8>(reqs, n_reqs, total, sh.block, counter, blocks, s);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <Mode M>
 cudaError_t launch_batch_mode(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, Accum acc,
-                              unsigned int* counter, int* blocks, cudaStream_t s)
+                              const LaunchShape& sh, unsigned int* counter, int* blocks, cudaStream_t s)
 {
     switch (acc) {
-    case Accum::F64: return launch_batch_typed<M, Accum::F64>(reqs, n_reqs, total, counter, blocks, s);
-    case Accum::Kahan: return launch_batch_typed<M, Accum::Kahan>(reqs, n_reqs, total, counter, blocks, s);
-    case Accum::F32: return launch_batch_typed<M, Accum::F32>(reqs, n_reqs, total, counter, blocks, s);
+    case Accum::F64: return launch_batch_unroll<M, Accum::F64>(reqs, n_reqs, total, sh, counter, blocks, s);
+    case Accum::Kahan: return launch_batch_unroll<M, Accum::Kahan>(reqs, n_reqs, total, sh, counter, blocks, s);
+    case Accum::F32: return launch_batch_unroll<M, Accum::F32>(reqs, n_reqs, total, sh, counter, blocks, s);
     }
     return cudaErrorInvalidValue;
 }
 }  // namespace
 
 cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
-                         unsigned int* counter, int* blocks, cudaStream_t s)
+                         const LaunchShape& shape, unsigned int* counter, int* blocks, cudaStream_t s)
 {
     if (total_items == 0 || n_reqs == 0)
         return cudaSuccess;
+    if (shape_error(shape))
+        return cudaErrorInvalidConfiguration;
     if (mode == Mode::Pairs)
-        return launch_batch_mode<Mode::Pairs>(reqs, n_reqs, total_items, acc, counter, blocks, s);
+        return launch_batch_mode<Mode::Pairs>(reqs, n_reqs, total_items, acc, shape, counter, blocks, s);
     if (mode == Mode::Cells)
-        return launch_batch_mode<Mode::Cells>(reqs, n_reqs, total_items, acc, counter, blocks, s);
+        return launch_batch_mode<Mode::Cells>(reqs, n_reqs, total_items, acc, shape, counter, blocks, s);
     return cudaErrorInvalidValue;
 }
 
@@ -844,13 +792,13 @@ cudaError_t launch_count(const ProjectArgs& a, Mode mode, cudaStream_t s)
     const uint64_t blocks = (uint64_t)a.view_groups * a.n_modules * a.tiles_per_vm;
     if (blocks == 0)
         return cudaSuccess;
-    if (blocks > 0x7fffffffull)
+    if (blocks > 0x7fffffffull || !block_ok(a))
         return cudaErrorInvalidConfiguration;
     const dim3 grid((unsigned)blocks);
     if (mode == Mode::Nearest)
-        count_kernel<Mode::Nearest><<<grid, kBlock, 0, s>>>(a);
+        count_kernel<Mode::Nearest><<<grid, a.block, 0, s>>>(a);
     else
-        count_kernel<Mode::Trilinear><<<grid, kBlock, 0, s>>>(a);
+        count_kernel<Mode::Trilinear><<<grid, a.block, 0, s>>>(a);
     return cudaGetLastError();
 }
 

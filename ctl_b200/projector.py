@@ -87,6 +87,11 @@ class Settings:
     accum: int = L.ACCUM_FP64
     storage: int = L.F32
     kernel: int = L.KERNEL_AUTO
+    # launch shape (0 = autotuned for the volume and detector, else the default)
+    views_per_block: int = 0
+    lanes_x: int = 0
+    block_rays: int = 0
+    unroll: int = 0
 
     def to_c(self) -> L.Settings:
         s = L.Settings()
@@ -98,7 +103,15 @@ class Settings:
         s.interp_mode = int(self.interp_mode)
         s.accum = int(self.accum)
         s.kernel = int(self.kernel)
+        s.views_per_block = int(self.views_per_block)
+        s.lanes_x = int(self.lanes_x)
+        s.block_rays = int(self.block_rays)
+        s.unroll = int(self.unroll)
         return s
+
+    def launch_shape(self) -> dict:
+        return {"views_per_block": self.views_per_block, "lanes_x": self.lanes_x,
+                "block_rays": self.block_rays, "unroll": self.unroll}
 
     @staticmethod
     def optimized_for(smallest_voxel_mm: float, pixel_dims_mm: Sequence[float]) -> "Settings":
@@ -488,8 +501,9 @@ class Context:
 
     def autotune(self, volume: Volume, pmats, channels: int, rows: int,
                  settings: Optional[Settings] = None, max_views: int = 8):
-        """Time the sample loops on a view subset; later KERNEL_AUTO calls with this
-        volume and detector use the fastest.  Returns (kernel, {name: ms})."""
+        """Time the sample loops on a view subset, then the launch shape of the
+        fastest; later KERNEL_AUTO calls with this volume and detector use them.
+        Returns (kernel, {loop name: ms with the default shape})."""
         settings = settings or Settings()
         P = _contig_f64(pmats)
         k = C.c_int(0)
@@ -499,6 +513,19 @@ class Context:
                                             int(P.shape[0]), int(P.shape[1]), int(channels), int(rows),
                                             int(max_views), C.byref(k), ms))
         return int(k.value), {"cells": ms[0], "pairs": ms[1], "gather": ms[2]}
+
+    def tuned_settings(self, volume: Volume, n_modules: int, channels: int, rows: int,
+                       settings: Optional[Settings] = None) -> Settings:
+        """The settings a projection of `volume` onto this detector runs with: the
+        sample loop and every launch-shape field resolved (ctlcu_tuned_settings)."""
+        settings = settings or Settings()
+        st = settings.to_c()
+        out = L.Settings()
+        self._check(self.lib.ctlcu_tuned_settings(self.h, volume.handle, C.byref(st), int(n_modules),
+                                                  int(channels), int(rows), C.byref(out)))
+        from dataclasses import replace
+        return replace(settings, kernel=out.kernel, views_per_block=out.views_per_block, lanes_x=out.lanes_x,
+                       block_rays=out.block_rays, unroll=out.unroll)
 
     def view_setup(self, pmats):
         P = np.ascontiguousarray(pmats, dtype=np.float64)

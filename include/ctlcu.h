@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CTLCU_ABI_VERSION 1
+#define CTLCU_ABI_VERSION 2  /* 2: launch-shape fields appended to ctlcu_settings */
 
 #if defined(__GNUC__)
 #define CTLCU_API __attribute__((visibility("default")))
@@ -103,6 +103,17 @@ typedef struct {
     int32_t interp_mode;        /* ctlcu_interp_mode */
     int32_t accum;              /* ctlcu_accum */
     int32_t kernel;             /* ctlcu_kernel: sample-loop variant (0 = automatic) */
+    /* Launch shape (no counterpart in the reference, whose OpenCL work size is
+     * one work-item per pixel, raycasterprojector.cpp:339-343).  0 = the
+     * autotuned value for this volume and detector (ctlcu_autotune), else the
+     * default in brackets.  Results do not depend on the first three; `unroll`
+     * changes only the FP32 rounding of the partial sums. */
+    int32_t views_per_block;    /* views sharing a thread block: 1, 2 or 4 [2] */
+    int32_t lanes_x;            /* warp patch along the channels: 4 (4x8 pixels) or 8 (8x4) [4] */
+    int32_t block_rays;         /* rays (threads) per block: 128, 256 or 512 [256]; the tile is
+                                   block_rays/views_per_block pixels, 16 channels wide from 128
+                                   pixels up, else 8 */
+    int32_t unroll;             /* cell/pair loops: samples per FP32 partial sum, 2, 4 or 8 [4] */
 } ctlcu_settings;
 
 /* One projection request of a batch: device pointers, see ctlcu_project_batch. */
@@ -203,15 +214,25 @@ CTLCU_API int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_s
 /*
  * Autotuner: times the sample loops that serve these settings (cell, pair and
  * gather loops for software trilinear interpolation without up-sampling) on
- * up to `max_views` evenly spaced views of the job (0 = 8), remembers the
- * fastest for later CTLCU_KERNEL_AUTO calls on this volume with the same
- * detector size and module count, keeps only the derived array the winner
- * reads, and returns it in *kernel.  ms_out (optional) receives the three
- * mean times in ms (cells, pairs, gather).  pmats: host or device.
+ * up to `max_views` evenly spaced views of the job (0 = 8), then, for the
+ * fastest loop, the launch shape one field at a time (views per block, warp
+ * patch, rays per block, and the unroll of the cell and pair loops), keeping
+ * each change that is faster.  Launch-shape fields set in `settings` stay
+ * fixed.  The result serves later calls on this volume with the same
+ * detector size and module count whose kernel is CTLCU_KERNEL_AUTO (loop and
+ * shape) or the tuned loop (shape); only the derived array the winner reads is
+ * kept.  *kernel receives the loop; ms_out (optional) the three loop times in
+ * ms (cells, pairs, gather) with the default shape.  pmats: host or device.
  */
 CTLCU_API int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
                              const double* pmats, uint32_t n_views, uint32_t n_modules, uint32_t channels,
                              uint32_t rows, uint32_t max_views, int* kernel, float* ms_out);
+
+/* The settings a projection of this volume with this detector size and module
+ * count runs with: *out = settings with the sample loop and every launch-shape
+ * field resolved (autotuned where a tuning exists, else the defaults). */
+CTLCU_API int ctlcu_tuned_settings(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings,
+                                   uint32_t n_modules, uint32_t channels, uint32_t rows, ctlcu_settings* out);
 
 /* Per-(view, module) packed QR (15 doubles: Q row-major, R00 R01 R02 R11 R12 R22)
  * and per-view source position (3 doubles), computed by the device setup

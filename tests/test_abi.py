@@ -30,7 +30,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     lib = L.load()
     for name in declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.ctlcu_abi_version() == 1
+    assert lib.ctlcu_abi_version() == L.ABI_VERSION == 2
 
 
 def test_binding_covers_the_header():
@@ -47,7 +47,7 @@ def test_only_the_c_abi_is_exported():
 
 def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(L.VolumeDesc) == 3 * 4 + 3 * 4 + 3 * 4 + 4
-    assert ctypes.sizeof(L.Settings) == 8 * 4
+    assert ctypes.sizeof(L.Settings) == 12 * 4
     assert ctypes.sizeof(L.Request) == 8 + 8 + 8 + 4 * 4
 
 
@@ -80,6 +80,30 @@ def test_default_settings_are_the_reference_defaults():
     assert abs(s.ray_sampling - 0.3) < 1e-7
     assert s.volume_upsampling == 1 and s.interpolate == 1
     assert s.interp_mode == L.INTERP_SOFTWARE and s.accum == L.ACCUM_FP64
+    # launch shape left to the autotuner / defaults
+    assert (s.views_per_block, s.lanes_x, s.block_rays, s.unroll) == (0, 0, 0, 0)
+
+
+def test_launch_shape_rules_mirror_the_kernel_tiling():
+    """The tile of a shape is block/views pixels, 16 channels wide from 128 pixels
+    up; a warp patch lanes_x x 32/lanes_x must tile it exactly (only 128 rays,
+    4 views and 4x8 patches do not fit: an 8x4 tile)."""
+    def tile(block, views):
+        p = block // views
+        tx = 16 if p >= 128 else 8
+        return tx, p // tx
+    bad = []
+    for block in (128, 256, 512):
+        for views in (1, 2, 4):
+            tx, ty = tile(block, views)
+            assert tx * ty == block // views
+            for lanes in (4, 8):
+                if ty % (32 // lanes) or tx % lanes:
+                    bad.append((block, views, lanes))
+                else:
+                    warps = block // 32 // views
+                    assert (tx // lanes) * (ty // (32 // lanes)) == warps
+    assert bad == [(128, 4, 4)]
 
 
 def test_bad_device_is_rejected_without_compute():
