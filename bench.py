@@ -384,7 +384,7 @@ def run_single_config(args, name):
              "cells_fp32": Settings(accum=L.ACCUM_FP32), "gather_fp64": Settings(kernel=L.KERNEL_GATHER),
              "texture_fp64": Settings(interp_mode=L.INTERP_TEXTURE)}
     storages = {"f32": L.F32, "bf16": L.BF16}
-    results = {}
+    results, shapes = {}, {}
     for sname, storage in storages.items():
         vol = ctx.volume(VoxelVolume(job.volume, job.voxel), storage)
         for fname, s in forms.items():
@@ -393,12 +393,20 @@ def run_single_config(args, name):
             ms = _time_device(lambda: ctx.project(vol, dP, job.channels, job.rows, s, out=out, stream=ctx.stream),
                               args.steps, args.warmup, stream)
             results[f"{sname}_{fname}"] = V / (statistics.mean(ms) / 1e3)
+        # the autotuned sample loop and launch shape (FP64 accumulation)
+        ctx.autotune(vol, job.pmats, job.channels, job.rows)
+        tuned = ctx.tuned_settings(vol, M, job.channels, job.rows)
+        ms = _time_device(lambda: ctx.project(vol, dP, job.channels, job.rows, Settings(), out=out,
+                                              stream=ctx.stream), args.steps, args.warmup, stream)
+        results[f"{sname}_tuned_fp64"] = V / (statistics.mean(ms) / 1e3)
+        shapes[sname] = dict(tuned.launch_shape(), loop={L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs",
+                                                          L.KERNEL_GATHER: "gather"}[tuned.kernel])
         if sname == "f32":
             samples = ctx.count_samples(vol, job.pmats, job.channels, job.rows)
         vol.release()
-    best = results["f32_cells_fp64"]
+    best = results["f32_tuned_fp64"]  # the automatic path once tuned
     ms = V / best * 1e3
-    extra = {"forms_views_per_s": results, "samples_per_step": samples,
+    extra = {"forms_views_per_s": results, "tuned": shapes, "samples_per_step": samples,
              "gsamples_per_s": samples / (ms / 1e3) / 1e9}
     if name == "c1" and not args.no_cpu_baseline:
         import oracle

@@ -214,11 +214,13 @@ CTLCU_API int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_s
 /*
  * Autotuner: times the sample loops that serve these settings (cell, pair and
  * gather loops for software trilinear interpolation without up-sampling) on
- * up to `max_views` evenly spaced views of the job (0 = 8), then, for the
- * fastest loop, the launch shape one field at a time (views per block, warp
- * patch, rays per block, and the unroll of the cell and pair loops), keeping
- * each change that is faster.  Launch-shape fields set in `settings` stay
- * fixed.  The result serves later calls on this volume with the same
+ * a contiguous run of views from the middle of the job (at least `max_views`,
+ * 0 = 8, lengthened until its rays fill the GPU about four times over, at most
+ * the job), then, for the fastest loop, the launch shape one field at a time
+ * (views per block, warp patch, rays per block, and the unroll of the cell and
+ * pair loops), keeping a change that is at least 1% faster; a final shape other
+ * than the default must win once more against it, timed afresh.  Launch-shape
+ * fields set in `settings` stay fixed.  The result serves later calls on this volume with the same
  * detector size and module count whose kernel is CTLCU_KERNEL_AUTO (loop and
  * shape) or the tuned loop (shape); only the derived array the winner reads is
  * kept.  *kernel receives the loop; ms_out (optional) the three loop times in
