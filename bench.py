@@ -48,9 +48,9 @@ N_VIEWS = 360
 METRIC = "projections/s at 256^3->512^2 (plain FP32)"
 WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
 # DRAM bytes (read + write) of one 360-view launch of the cell loop on this
-# workload, from one ncu capture (profiles/project_kernel_cells_256cubed_to_512sq_dram.md),
+# workload, from one ncu capture (profiles/cells_kernel_256cubed_to_512sq_dram.md),
 # with the launch shape it was captured at (views per block, lanes_x, rays per block, unroll)
-CELLS_TRAFFIC_BYTES = 7.90e9 + 0.75271e9
+CELLS_TRAFFIC_BYTES = 7.914174208e9 + 0.761463552e9
 CELLS_TRAFFIC_SHAPE = (2, 4, 256, 4)
 
 
