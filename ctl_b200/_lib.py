@@ -131,6 +131,9 @@ SIGNATURES = [
                                        C.c_void_p, C.c_void_p]),
     ("ctlcu_spectral_combine", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ctlcu_spectral_combine_noisy", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                               C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                               C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("ctlcu_den_write", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                   C.c_uint32, C.c_void_p]),
     ("ctlcu_den_header", C.c_int, [C.c_char_p, C.POINTER(C.c_uint32 * 3), C.POINTER(C.c_uint32)]),

@@ -1699,6 +1699,75 @@ int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs, uint32_t
     return CTLCU_OK;
 }
 
+int ctlcu_spectral_combine_noisy(ctlcu_ctx* ctx, const float* material_projs, uint32_t n_materials, uint32_t n_views,
+                                 uint32_t n_modules, uint64_t pixels_per_module, const float* mu_per_mm,
+                                 const double* intensities, const float* response, uint32_t n_bins,
+                                 const double* total_intensity, const float* i0_per_bin_module, uint64_t seed,
+                                 float* out, void* stream)
+{
+    TraceRange trace_("ctlcu_spectral_combine_noisy");
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!material_projs || !mu_per_mm || !intensities || !total_intensity || !i0_per_bin_module || !out ||
+        !n_materials || !n_bins)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "NULL argument, no materials or no energy bins");
+    if (n_views == 0 || n_modules == 0 || pixels_per_module == 0)
+        return CTLCU_OK;
+    if (pixels_per_module > 0xffffffffull / n_modules)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many pixels per view");
+    cudaSetDevice(ctx->device);
+    if (!is_device_ptr(material_projs) || !is_device_ptr(out))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "projections must be device memory");
+    // spectraleffectsextension.cpp:373: a bin without flux is skipped; poissonnoiseextension.cpp:160:
+    // projections whose i0 sums to zero pass the noise step unchanged
+    std::vector<int> skip(n_bins, 0), quiet(n_bins, 0);
+    for (uint32_t b = 0; b < n_bins; ++b) {
+        double s = 0.0, q = 0.0;
+        for (uint32_t v = 0; v < n_views; ++v)
+            s += intensities[(size_t)b * n_views + v];
+        for (uint32_t k = 0; k < n_modules; ++k)
+            q += i0_per_bin_module[(size_t)b * n_modules + k];
+        skip[b] = std::fabs(s) <= 1e-12;
+        quiet[b] = std::fabs(q) <= 1e-12;
+    }
+    std::vector<float> resp(n_bins, 1.0f);
+    if (response)
+        std::copy(response, response + n_bins, resp.begin());
+    const size_t b_mu = sizeof(float) * n_bins * n_materials, b_int = sizeof(double) * n_bins * n_views,
+                 b_resp = sizeof(float) * n_bins, b_flag = sizeof(int) * n_bins, b_tot = sizeof(double) * n_views,
+                 b_i0 = sizeof(float) * n_bins * n_modules;
+    const size_t o_int = 0, o_tot = o_int + b_int, o_mu = o_tot + b_tot, o_resp = o_mu + b_mu,
+                 o_skip = o_resp + b_resp, o_quiet = o_skip + b_flag, o_i0 = o_quiet + b_flag;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    char* buf = nullptr;
+    CU_TRY(ctx, cudaMallocAsync((void**)&buf, o_i0 + b_i0, st));
+    const std::pair<size_t, std::pair<const void*, size_t>> copies[] = {
+        { o_int, { intensities, b_int } }, { o_tot, { total_intensity, b_tot } },
+        { o_mu, { mu_per_mm, b_mu } },     { o_resp, { resp.data(), b_resp } },
+        { o_skip, { skip.data(), b_flag } }, { o_quiet, { quiet.data(), b_flag } },
+        { o_i0, { i0_per_bin_module, b_i0 } } };
+    cudaError_t e = cudaSuccess;
+    for (const auto& c : copies)
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(buf + c.first, c.second.first, c.second.second, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = launch_spectral_noisy(material_projs, n_materials, n_views, n_modules, (uint32_t)pixels_per_module,
+                                  (const float*)(buf + o_mu), (const double*)(buf + o_int),
+                                  (const float*)(buf + o_resp), (const int*)(buf + o_skip),
+                                  (const int*)(buf + o_quiet), n_bins, (const double*)(buf + o_tot),
+                                  (const float*)(buf + o_i0), seed, out, st);
+    // the host vectors die on return: the copies out of them must be done
+    const cudaError_t w = cudaStreamSynchronize(st);
+    cudaFreeAsync(buf, st);
+    if (e == cudaSuccess)
+        e = w;
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "noisy spectral combine: %s", cudaGetErrorString(e));
+    ++ctx->launches;
+    return CTLCU_OK;
+}
+
 int ctlcu_combine_linear(ctlcu_ctx* ctx, const float* slope_proj, const float* offset_proj, const double* times,
                          uint32_t n_views, uint64_t values_per_view, float* out, void* stream)
 {

@@ -221,6 +221,53 @@ __global__ void spectral_kernel(const float* __restrict__ proj, uint32_t n_mater
     }
 }
 
+// SpectralEffectsExtension over a nested projector + PoissonNoiseExtension
+// (spectraleffectsextension.cpp:285-314, :368-391): per energy bin, every
+// material's projection mu[b][m] * proj_m gets its own noise draw with the
+// bin's photon count i0[b][module], exactly as poisson_kernel would draw it
+// with seed + c, where c counts the (bin, material) projections of the bins not
+// skipped in loop order (one nested project() call each).  The noisy
+// extinctions of a bin are summed over the materials, and the bins combined in
+// the intensity domain as spectral_kernel does.  `quiet[b]`: the bin's i0 sums
+// to zero, and the nested noise step leaves its projections as they are
+// (poissonnoiseextension.cpp:160).
+__global__ void spectral_noisy_kernel(const float* __restrict__ proj, uint32_t n_materials, uint32_t n_views,
+                                      uint32_t n_modules, uint32_t ppm, const float* __restrict__ mu,
+                                      const double* __restrict__ intensity, const float* __restrict__ response,
+                                      const int* __restrict__ skip, const int* __restrict__ quiet, uint32_t n_bins,
+                                      const double* __restrict__ total, const float* __restrict__ i0, uint64_t seed,
+                                      float* __restrict__ out)
+{
+    const uint64_t per_view = (uint64_t)n_modules * ppm;
+    const uint64_t n = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(i / per_view);
+        const uint32_t pix = (uint32_t)(i - (uint64_t)v * per_view);
+        const uint32_t module = pix / ppm;
+        float sum = 0.0f;
+        uint64_t call = 0;
+        for (uint32_t b = 0; b < n_bins; ++b) {
+            if (skip[b])
+                continue;
+            const float i0m = i0[(uint64_t)b * n_modules + module];
+            float e = 0.0f;
+            for (uint32_t m = 0; m < n_materials; ++m, ++call) {
+                const float em = proj[(uint64_t)m * n + i] * mu[(uint64_t)b * n_materials + m];
+                if (quiet[b]) {
+                    e += em;
+                    continue;
+                }
+                const uint64_t sc = seed + call;
+                const double lam = (double)i0m * exp(-(double)em);
+                Stream s{ pix, v, 0u, (uint32_t)sc, (uint32_t)(sc >> 32) };
+                e += logf(i0m / noisy_count(lam, s));
+            }
+            sum += (float)intensity[(uint64_t)b * n_views + v] * expf(-e) * response[b];
+        }
+        out[i] = logf((float)total[v] / sum);
+    }
+}
+
 unsigned grid_for_elements(uint64_t n)
 {
     uint64_t b = (n + 255) / 256;
@@ -250,6 +297,20 @@ cudaError_t launch_spectral(const float* proj, uint32_t n_materials, uint64_t pe
         return cudaSuccess;
     spectral_kernel<<<grid_for_elements(n), 256, 0, s>>>(proj, n_materials, per_view, n_views, mu, intensity, response,
                                                           skip, n_bins, total, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spectral_noisy(const float* proj, uint32_t n_materials, uint32_t n_views, uint32_t n_modules,
+                                  uint32_t ppm, const float* mu, const double* intensity, const float* response,
+                                  const int* skip, const int* quiet, uint32_t n_bins, const double* total,
+                                  const float* i0, uint64_t seed, float* out, cudaStream_t s)
+{
+    const uint64_t n = (uint64_t)n_modules * ppm * n_views;
+    if (n == 0)
+        return cudaSuccess;
+    spectral_noisy_kernel<<<grid_for_elements(n), 256, 0, s>>>(proj, n_materials, n_views, n_modules, ppm, mu,
+                                                                intensity, response, skip, quiet, n_bins, total, i0,
+                                                                seed, out);
     return cudaGetLastError();
 }
 

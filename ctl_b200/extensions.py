@@ -185,23 +185,34 @@ class DynamicProjectorExtension:
 
 
 class SpectralEffectsExtension:
-    """SpectralEffectsExtension, linear case (projectors/spectraleffectsextension.cpp:215-278):
-    the materials' density volumes projected in one batched launch, then every energy bin
-    combined per pixel on the device (ctlcu_spectral_combine).
+    """SpectralEffectsExtension (projectors/spectraleffectsextension.cpp): the materials'
+    density volumes projected in one batched launch, then every energy bin combined per
+    pixel on the device.
+
+    Linear case (:215-278; ctlcu_spectral_combine): the nested projector is linear.
+    Around a nested PoissonNoiseExtension (the non-linear case, :285-314, :368-391;
+    ctlcu_spectral_combine_noisy): the reference projects every material's attenuation
+    volume per energy bin through projector | noise; here the density projections are
+    scaled per bin (the projector is linear) and only the noise runs per (bin, material).
 
     The spectral inputs come from CTL's models, evaluated by the caller:
       mu_per_mm  [bins][materials]: meanMassAttenuationCoeff(E_b, binWidth) * 0.1 (cm -> mm)
       intensities [bins][views]:   RadiationEncoder bin intensities per view
       total_intensity [views]:     RadiationEncoder::totalIntensity()
-      response [bins] or None:     the detector's spectral response model at E_b"""
+      response [bins] or None:     the detector's spectral response model at E_b
+      photons_per_pixel [bins][modules] or None: the nested PoissonNoiseExtension's i0 in
+                                   each bin (photonsPerPixel with the bin's flux); None for
+                                   the linear case
+      fixed_seed:                  the nested noise extension's fixed seed (None: random)"""
 
     def __init__(self, ctx: Context, settings: Optional[Settings] = None):
         self.ctx = ctx
         self.settings = settings or Settings()
         self._pm = None
+        self._calls = 0
 
     def configure(self, pmats, channels: int, rows: int, mu_per_mm, intensities, total_intensity,
-                  response=None) -> None:
+                  response=None, photons_per_pixel=None, fixed_seed: Optional[int] = None) -> None:
         self._pm = pmats
         self._dims = (int(channels), int(rows))
         self.mu = np.ascontiguousarray(mu_per_mm, np.float32)
@@ -209,11 +220,24 @@ class SpectralEffectsExtension:
         self.total = np.ascontiguousarray(total_intensity, np.float64)
         self.response = None if response is None else np.ascontiguousarray(response, np.float32)
         B, M = self.mu.shape
-        V = int(pmats.shape[0])
+        V, Mod = int(pmats.shape[0]), int(pmats.shape[1])
         if self.intensities.shape != (B, V) or self.total.shape != (V,):
             raise ValueError("intensities must be [bins][views] and total_intensity [views]")
         if self.response is not None and self.response.shape != (B,):
             raise ValueError("response must hold one value per bin")
+        self.i0 = None if photons_per_pixel is None else np.ascontiguousarray(photons_per_pixel, np.float32)
+        if self.i0 is not None and self.i0.shape != (B, Mod):
+            raise ValueError("photons_per_pixel must be [bins][modules]")
+        self.fixed_seed = fixed_seed
+
+    def is_linear(self) -> bool:
+        return self.i0 is None
+
+    def nested_calls(self) -> int:
+        """Projections the reference makes through the nested chain per project():
+        materials x bins not skipped (bins whose intensities sum to zero)."""
+        live = int((np.abs(self.intensities.sum(axis=1)) > 1e-12).sum())
+        return live * int(self.mu.shape[1])
 
     def project(self, material_densities: Sequence[VoxelVolume]):
         import torch
@@ -233,12 +257,24 @@ class SpectralEffectsExtension:
             from .projector import _ptr
             import ctypes as C
             stream = self.ctx._stream_for(0, out)
-            self.ctx._check(self.ctx.lib.ctlcu_spectral_combine(
-                self.ctx.h, C.c_void_p(_ptr(projs)), M, V, Mod * R * C_, C.c_void_p(self.mu.ctypes.data),
-                C.c_void_p(self.intensities.ctypes.data),
-                C.c_void_p(self.response.ctypes.data if self.response is not None else None),
-                int(self.mu.shape[0]), C.c_void_p(self.total.ctypes.data), C.c_void_p(_ptr(out)),
-                C.c_void_p(stream or None)))
+            resp = C.c_void_p(self.response.ctypes.data if self.response is not None else None)
+            if self.i0 is None:
+                self.ctx._check(self.ctx.lib.ctlcu_spectral_combine(
+                    self.ctx.h, C.c_void_p(_ptr(projs)), M, V, Mod * R * C_, C.c_void_p(self.mu.ctypes.data),
+                    C.c_void_p(self.intensities.ctypes.data), resp, int(self.mu.shape[0]),
+                    C.c_void_p(self.total.ctypes.data), C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
+                return out
+            if self.fixed_seed is not None:
+                seed = self.fixed_seed + self._calls  # the nested extension's next call
+            else:
+                seed = int.from_bytes(np.random.bytes(8), "little")
+            self._calls += self.nested_calls()
+            self.last_seed = seed
+            self.ctx._check(self.ctx.lib.ctlcu_spectral_combine_noisy(
+                self.ctx.h, C.c_void_p(_ptr(projs)), M, V, Mod, R * C_, C.c_void_p(self.mu.ctypes.data),
+                C.c_void_p(self.intensities.ctypes.data), resp, int(self.mu.shape[0]),
+                C.c_void_p(self.total.ctypes.data), C.c_void_p(self.i0.ctypes.data), C.c_uint64(seed % (1 << 64)),
+                C.c_void_p(_ptr(out)), C.c_void_p(stream or None)))
             return out
         finally:
             torch.cuda.synchronize()

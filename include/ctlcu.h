@@ -420,6 +420,28 @@ CTLCU_API int ctlcu_spectral_combine(ctlcu_ctx* ctx, const float* material_projs
                                      const double* intensities, const float* response, uint32_t n_bins,
                                      const double* total_intensity, float* out, void* stream);
 
+/* SpectralEffectsExtension around a non-linear nested chain, projector | PoissonNoiseExtension
+ * (projectors/spectraleffectsextension.cpp:285-314, :368-391).  The reference projects, per energy
+ * bin, each material's attenuation volume mu_m(E_b) * density_m through the nested chain, so each
+ * (bin, material) projection gets its own noise with the bin's photon count.  The projector is
+ * linear, so that projection is mu_per_mm[b][m] * material_projs[m]: one projection per material
+ * replaces bins x materials, and only the noise runs per (bin, material).  Per pixel of view v and
+ * module k:
+ *   e'_bm = log(i0[b][k] / n_bm),  n_bm ~ Poisson(i0[b][k] exp(-mu_per_mm[b][m] proj_m))
+ *   out   = log(total_intensity[v] / sum_b intensities[b][v] exp(-sum_m e'_bm) response[b])
+ * The draw for (b, m) is ctlcu_poisson_noise's with seed + c, c counting the (bin, material)
+ * projections of the bins not skipped in the reference's loop order (a fixed-seed noise
+ * extension's successive calls).  Bins whose intensities sum to zero are skipped; a bin whose i0
+ * sums to zero passes without noise.  i0_per_bin_module [bin][module] and the other spectral
+ * inputs as for ctlcu_spectral_combine, host memory; material_projs [material][view][module]
+ * [pixel] and out device memory.  Returns when done. */
+CTLCU_API int ctlcu_spectral_combine_noisy(ctlcu_ctx* ctx, const float* material_projs, uint32_t n_materials,
+                                           uint32_t n_views, uint32_t n_modules, uint64_t pixels_per_module,
+                                           const float* mu_per_mm, const double* intensities,
+                                           const float* response, uint32_t n_bins,
+                                           const double* total_intensity, const float* i0_per_bin_module,
+                                           uint64_t seed, float* out, void* stream);
+
 /*
  * No counterpart in the reference.  ctlcu_project for callers that cannot
  * allocate device memory while they run: a real-time loop that reserved all
