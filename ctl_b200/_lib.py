@@ -71,6 +71,15 @@ class TrajectoryDesc(C.Structure):
                 ("line_length_mm", C.c_double), ("line_fraction", C.c_double)]
 
 
+SATURATION_LINEAR, SATURATION_SPLINE = 0, 1
+SATURATION_EXTINCTION, SATURATION_PHOTON_COUNT, SATURATION_INTENSITY = 0, 1, 2
+
+
+class SaturationModel(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("a", C.c_float), ("b", C.c_float), ("soft_a", C.c_float),
+                ("soft_b", C.c_float)]
+
+
 class Request(C.Structure):
     _fields_ = [("volume", C.c_uint64), ("pmats", C.c_void_p), ("out", C.c_void_p),
                 ("n_views", C.c_uint32), ("n_modules", C.c_uint32), ("channels", C.c_uint32),
@@ -131,6 +140,8 @@ SIGNATURES = [
                                        C.c_void_p, C.c_void_p]),
     ("ctlcu_spectral_combine", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ctlcu_detector_saturation", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int32,
+                                            C.POINTER(SaturationModel), C.c_void_p, C.c_void_p]),
     ("ctlcu_spectral_combine_noisy", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                                C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                                C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),

@@ -1948,6 +1948,50 @@ int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t 
     });
 }
 
+int ctlcu_detector_saturation(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t n_modules,
+                              uint64_t pixels_per_module, int32_t domain, const ctlcu_saturation_model* model,
+                              const float* scale_per_view_module, void* stream)
+{
+    TraceRange trace_("ctlcu_detector_saturation");
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!data || !model)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "data or model is NULL");
+    if (domain < CTLCU_SATURATION_EXTINCTION || domain > CTLCU_SATURATION_INTENSITY)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown saturation domain %d", domain);
+    if (model->kind != CTLCU_SATURATION_LINEAR && model->kind != CTLCU_SATURATION_SPLINE)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown saturation model %d", model->kind);
+    if (model->kind == CTLCU_SATURATION_SPLINE && !(model->soft_a > 0.0f && model->soft_b > 0.0f))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "spline softening must be positive (%g, %g)",
+                    (double)model->soft_a, (double)model->soft_b);
+    if (domain != CTLCU_SATURATION_EXTINCTION && !scale_per_view_module)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "the photon count and intensity domains need the per-view, "
+                                                     "per-module photon counts");
+    if (n_views == 0 || n_modules == 0 || pixels_per_module == 0)
+        return CTLCU_OK;
+    if (pixels_per_module > (1ull << 40) / ((uint64_t)n_views * n_modules))
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many values");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(float) * pixels_per_module * n_modules * n_views;
+    const ctlcu_saturation_model m = *model;
+    return on_device_data(ctx, data, bytes, stream, "detector saturation", [&](float* d, cudaStream_t st) {
+        float* ds = nullptr;
+        cudaError_t e = cudaSuccess;
+        if (domain != CTLCU_SATURATION_EXTINCTION) {
+            const size_t sb = sizeof(float) * (size_t)n_views * n_modules;
+            e = cudaMallocAsync((void**)&ds, sb, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ds, scale_per_view_module, sb, cudaMemcpyHostToDevice, st);
+        }
+        if (e == cudaSuccess)
+            e = launch_saturation(d, n_views, n_modules, pixels_per_module, domain, m, ds, st);
+        if (ds)
+            cudaFreeAsync(ds, st);
+        return e;
+    });
+}
+
 int ctlcu_encode_geometry(ctlcu_ctx* ctx, const ctlcu_detector_desc* detector,
                           const ctlcu_trajectory_desc* trajectory, uint32_t n_views, double* pmats, void* stream)
 {

@@ -263,6 +263,8 @@ cudaError_t launch_combine_linear(const float* slope, const float* offset, const
 cudaError_t launch_spectral(const float* proj, uint32_t n_materials, uint64_t per_view, uint32_t n_views,
                             const float* mu, const double* intensity, const float* response, const int* skip,
                             uint32_t n_bins, const double* total, float* out, cudaStream_t s);
+cudaError_t launch_saturation(float* data, uint32_t n_views, uint32_t n_modules, uint64_t ppm, int domain,
+                              const ctlcu_saturation_model& model, const float* scale, cudaStream_t s);
 cudaError_t launch_spectral_noisy(const float* proj, uint32_t n_materials, uint32_t n_views, uint32_t n_modules,
                                   uint32_t ppm, const float* mu, const double* intensity, const float* response,
                                   const int* skip, const int* quiet, uint32_t n_bins, const double* total,

@@ -221,6 +221,58 @@ __global__ void spectral_kernel(const float* __restrict__ proj, uint32_t n_mater
     }
 }
 
+// DetectorSaturationLinearModel::valueAt / DetectorSaturationSplineModel::valueAt
+// (models/detectorsaturationmodels.cpp), in the reference's FP32 operation order,
+// written with round-to-nearest intrinsics so that no multiply-add is contracted.
+__device__ __forceinline__ float saturation_value(float x, const ctlcu_saturation_model& m)
+{
+    if (m.kind == CTLCU_SATURATION_LINEAR)
+        return x < m.a ? m.a : (x > m.b ? m.b : x);
+    const float s1s = __fsub_rn(m.a, m.soft_a), s1e = __fadd_rn(m.a, m.soft_a);
+    const float s2s = __fsub_rn(m.b, m.soft_b), s2e = __fadd_rn(m.b, m.soft_b);
+    if (x < s1s)
+        return m.a;
+    if (x < s1e) {
+        // 1/(4 sa) x^2 - (a - sa)/(2 sa) x + (a + sa)^2/(4 sa)
+        const float t1 = __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(4.0f, m.soft_a)), __fmul_rn(x, x));
+        const float t2 = __fmul_rn(__fdiv_rn(s1s, __fmul_rn(2.0f, m.soft_a)), x);
+        const float t3 = __fdiv_rn(__fmul_rn(s1e, s1e), __fmul_rn(4.0f, m.soft_a));
+        return __fadd_rn(__fsub_rn(t1, t2), t3);
+    }
+    if (x < s2s)
+        return x;
+    if (x < s2e) {
+        // -1/(4 sb) x^2 + (b + sb)/(2 sb) x - (b - sb)^2/(4 sb)
+        const float t1 = __fmul_rn(__fdiv_rn(-1.0f, __fmul_rn(4.0f, m.soft_b)), __fmul_rn(x, x));
+        const float t2 = __fmul_rn(__fdiv_rn(s2e, __fmul_rn(2.0f, m.soft_b)), x);
+        const float t3 = __fdiv_rn(__fmul_rn(s2s, s2s), __fmul_rn(4.0f, m.soft_b));
+        return __fsub_rn(__fadd_rn(t1, t2), t3);
+    }
+    return m.b;
+}
+
+// DetectorSaturationExtension::processExtinctions / processCounts / processIntensities
+// (projectors/detectorsaturationextension.cpp:96-226); `scale` [view][module] is the
+// photon count (or count x mean energy) the extinctions refer to, unused in the
+// extinction domain.
+__global__ void saturation_kernel(float* __restrict__ data, uint32_t n_views, uint32_t n_modules, uint64_t ppm,
+                                  int domain, ctlcu_saturation_model m, const float* __restrict__ scale)
+{
+    const uint64_t per_view = (uint64_t)n_modules * ppm;
+    const uint64_t n = per_view * n_views;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (domain == CTLCU_SATURATION_EXTINCTION) {
+            data[i] = saturation_value(data[i], m);
+            continue;
+        }
+        const uint32_t v = (uint32_t)(i / per_view);
+        const uint32_t k = (uint32_t)((i - (uint64_t)v * per_view) / ppm);
+        const float s = scale[(uint64_t)v * n_modules + k];
+        const float x = saturation_value(__fmul_rn(s, expf(-data[i])), m);
+        data[i] = logf(__fdiv_rn(s, x));
+    }
+}
+
 // SpectralEffectsExtension over a nested projector + PoissonNoiseExtension
 // (spectraleffectsextension.cpp:285-314, :368-391): per energy bin, every
 // material's projection mu[b][m] * proj_m gets its own noise draw with the
@@ -297,6 +349,16 @@ cudaError_t launch_spectral(const float* proj, uint32_t n_materials, uint64_t pe
         return cudaSuccess;
     spectral_kernel<<<grid_for_elements(n), 256, 0, s>>>(proj, n_materials, per_view, n_views, mu, intensity, response,
                                                           skip, n_bins, total, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_saturation(float* data, uint32_t n_views, uint32_t n_modules, uint64_t ppm, int domain,
+                              const ctlcu_saturation_model& model, const float* scale, cudaStream_t s)
+{
+    const uint64_t n = (uint64_t)n_modules * ppm * n_views;
+    if (n == 0)
+        return cudaSuccess;
+    saturation_kernel<<<grid_for_elements(n), 256, 0, s>>>(data, n_views, n_modules, ppm, domain, model, scale);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,13 @@ one launch each of geometry, projection and reduction:
     domain, or extinction domain with the low-extinction approximation).
   PoissonNoiseExtension (projectors/poissonnoiseextension.cpp:35-68):
     ctlcu_poisson_noise on the device result.
+  DynamicProjectorExtension over a LinearDynamicVolume: two projections and
+    ctlcu_combine_linear.
+  SpectralEffectsExtension: one batched projection of the material densities and
+    ctlcu_spectral_combine (linear), or ctlcu_spectral_combine_noisy around a
+    nested PoissonNoiseExtension.
+  DetectorSaturationExtension (projectors/detectorsaturationextension.cpp:96-226):
+    ctlcu_detector_saturation on the device result.
 """
 from __future__ import annotations
 
@@ -308,3 +315,62 @@ class PoissonNoiseExtension:
         self._calls += 1
         i0 = np.broadcast_to(self.i0, (int(out.shape[1]),))
         return self.ctx.poisson_noise(out, i0, seed)
+
+
+def linear_saturation(lower_cap: float, upper_cap: float):
+    """DetectorSaturationLinearModel(lowerCap, upperCap) (models/detectorsaturationmodels.cpp)."""
+    from . import _lib as L
+    return L.SaturationModel(L.SATURATION_LINEAR, float(lower_cap), float(upper_cap), 0.0, 0.0)
+
+
+def spline_saturation(lower_cap: float, upper_cap: float, soft_lower: float, soft_upper: Optional[float] = None):
+    """DetectorSaturationSplineModel(lowerCap, upperCap, softLower[, softUpper])."""
+    from . import _lib as L
+    su = soft_lower if soft_upper is None else soft_upper
+    return L.SaturationModel(L.SATURATION_SPLINE, float(lower_cap), float(upper_cap), float(soft_lower), float(su))
+
+
+class DetectorSaturationExtension:
+    """DetectorSaturationExtension (projectors/detectorsaturationextension.cpp:96-226) around
+    a B200 projector or extension: the nested projection, then the detector's saturation
+    model applied on the device in its domain (ctlcu_detector_saturation).
+
+      model:             linear_saturation(...) or spline_saturation(...)
+      domain:            L.SATURATION_EXTINCTION, _PHOTON_COUNT or _INTENSITY
+                         (AbstractDetector::saturationModelType())
+      photons_per_pixel: [views][modules] or [modules]: SimpleCTSystem::photonsPerPixel()
+                         after prepareView, for the photon count and intensity domains
+      mean_energy:       [views] or scalar (keV): the centroid of each view's spectrum,
+                         for the intensity domain (i0 = count x mean energy)"""
+
+    def __init__(self, nested, model, domain: int, photons_per_pixel=None, mean_energy=None):
+        from . import _lib as L
+        if not isinstance(getattr(nested, "ctx", None), Context):
+            raise TypeError("the nested projector must be a B200 projector or extension (with a Context)")
+        if domain != L.SATURATION_EXTINCTION and photons_per_pixel is None:
+            raise ValueError("the photon count and intensity domains need photons_per_pixel")
+        if domain == L.SATURATION_INTENSITY and mean_energy is None:
+            raise ValueError("the intensity domain needs the spectrum's mean energy")
+        self.nested, self.ctx = nested, nested.ctx
+        self.model, self.domain = model, int(domain)
+        self.n0 = None if photons_per_pixel is None else np.asarray(photons_per_pixel, np.float32)
+        self.mean_energy = None if mean_energy is None else np.asarray(mean_energy, np.float32)
+
+    def is_linear(self) -> bool:
+        return False
+
+    def scale(self, n_views: int, n_modules: int):
+        """The per-[view][module] count (or intensity) the extinctions refer to."""
+        from . import _lib as L
+        if self.domain == L.SATURATION_EXTINCTION:
+            return None
+        n0 = np.broadcast_to(self.n0, (n_views, n_modules)).astype(np.float32)
+        if self.domain == L.SATURATION_INTENSITY:
+            e = np.broadcast_to(self.mean_energy, (n_views,)).astype(np.float32)
+            n0 = (n0 * e[:, None]).astype(np.float32)   # RadiationEncoder count x centroid, in float
+        return n0
+
+    def project(self, volume):
+        out = self.nested.project(volume)
+        V, M = int(out.shape[0]), int(out.shape[1])
+        return self.ctx.detector_saturation(out, self.model, self.domain, self.scale(V, M))

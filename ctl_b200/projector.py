@@ -438,6 +438,23 @@ class Context:
                                                  C.c_void_p(stream or None)))
         return data
 
+    def detector_saturation(self, data, model: "L.SaturationModel", domain: int, scale=None, stream: int = 0):
+        """DetectorSaturationExtension's step on extinction data [view][module][rows][channels]
+        in place.  domain: L.SATURATION_EXTINCTION / _PHOTON_COUNT / _INTENSITY; scale: the
+        photon count (or count x mean energy) per [view][module] for the last two."""
+        data = self._inplace_f32(data)
+        V, M = int(data.shape[0]), int(data.shape[1])
+        ppm = int(np.prod(tuple(data.shape[2:])))
+        arr = None
+        if scale is not None:
+            arr = np.ascontiguousarray(np.broadcast_to(np.asarray(scale, np.float32), (V, M)))
+        stream = self._stream_for(stream, data)
+        self._check(self.lib.ctlcu_detector_saturation(self.h, C.c_void_p(_ptr(data)), V, M, ppm, int(domain),
+                                                       C.byref(model),
+                                                       C.c_void_p(arr.ctypes.data if arr is not None else None),
+                                                       C.c_void_p(stream or None)))
+        return data
+
     def project_volume(self, vol: VoxelVolume, pmats, channels: int, rows: int,
                        settings: Optional[Settings] = None, out=None):
         """One-shot: upload, project, release (the reference's per-call semantics)."""

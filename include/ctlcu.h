@@ -277,6 +277,38 @@ CTLCU_API int ctlcu_poisson_noise(ctlcu_ctx* ctx, float* data, uint32_t n_views,
                                   uint32_t pixels_per_module, const float* i0_per_module, uint64_t seed,
                                   void* stream);
 
+/* Detector saturation models (models/detectorsaturationmodels.cpp): LINEAR clamps to [a, b];
+ * SPLINE is the identity between a + soft_a and b - soft_b, constant a below a - soft_a and b
+ * above b + soft_b, with the reference's quadratic splines in between. */
+typedef enum { CTLCU_SATURATION_LINEAR = 0, CTLCU_SATURATION_SPLINE = 1 } ctlcu_saturation_kind;
+typedef struct {
+    int32_t kind;          /* ctlcu_saturation_kind */
+    float a, b;            /* lower and upper cap */
+    float soft_a, soft_b;  /* SPLINE: half widths of the lower and upper transitions (> 0) */
+} ctlcu_saturation_model;
+
+/* Domain the saturation model acts in (AbstractDetector::SaturationModelType). */
+typedef enum {
+    CTLCU_SATURATION_EXTINCTION = 0,
+    CTLCU_SATURATION_PHOTON_COUNT = 1,
+    CTLCU_SATURATION_INTENSITY = 2
+} ctlcu_saturation_domain;
+
+/*
+ * DetectorSaturationExtension (projectors/detectorsaturationextension.cpp:96-226) on extinction
+ * data [view][module][pixel], in place, in FP32 as the reference computes it:
+ *   extinction domain:         p = model(p)
+ *   photon count / intensity:  x = s[v][k] exp(-p); x = model(x); p = log(s[v][k] / x)
+ * where s[view][module] (host memory) is the incident photon count per pixel in the photon
+ * count domain (SimpleCTSystem::photonsPerPixel after prepareView) and that count times the
+ * mean energy of the view's spectrum in the intensity domain; NULL in the extinction domain.
+ * data: device (asynchronous on `stream`) or host memory (returns when done).
+ */
+CTLCU_API int ctlcu_detector_saturation(ctlcu_ctx* ctx, float* data, uint32_t n_views, uint32_t n_modules,
+                                        uint64_t pixels_per_module, int32_t domain,
+                                        const ctlcu_saturation_model* model, const float* scale_per_view_module,
+                                        void* stream);
+
 /* ---- DEN files ---------------------------------------------------------------------------- */
 
 /*

@@ -161,3 +161,34 @@ def poisson_noise_reference(extinction, i0_per_module, seed):
     C.CDLL(path).ref_poisson_noise(x.ctypes.data_as(fp), C.c_uint(V), C.c_uint(M), C.c_uint(ppm),
                                    i0.ctypes.data_as(fp), C.c_uint(seed))
     return x
+
+
+def saturation_value(x, kind, a, b, soft_a=0.0, soft_b=0.0):
+    """DetectorSaturationLinearModel::valueAt / DetectorSaturationSplineModel::valueAt and
+    spline1/spline2 (models/detectorsaturationmodels.cpp:27-35, :108-127, :294-307), FP32,
+    one rounding per operation in the reference's order."""
+    f = np.float32
+    x = np.asarray(x, np.float32)
+    a, b, sa, sb = f(a), f(b), f(soft_a), f(soft_b)
+    if kind == 0:
+        return np.where(x < a, a, np.where(x > b, b, x)).astype(np.float32)
+    s1s, s1e, s2s, s2e = f(a - sa), f(a + sa), f(b - sb), f(b + sb)
+    with np.errstate(over="ignore", invalid="ignore"):
+        sp1 = (f(1.0) / (f(4.0) * sa)) * (x * x) - (s1s / (f(2.0) * sa)) * x + (s1e * s1e) / (f(4.0) * sa)
+        sp2 = (f(-1.0) / (f(4.0) * sb)) * (x * x) + (s2e / (f(2.0) * sb)) * x - (s2s * s2s) / (f(4.0) * sb)
+    out = np.where(x < s1s, a, np.where(x < s1e, sp1, np.where(x < s2s, x, np.where(x < s2e, sp2, b))))
+    return out.astype(np.float32)
+
+
+def detector_saturation(extinction, kind, a, b, soft_a, soft_b, domain, scale=None):
+    """DetectorSaturationExtension::processExtinctions / processCounts / processIntensities
+    (projectors/detectorsaturationextension.cpp:118-226) on [V, M, ...] extinctions, FP32:
+    domain 0 applies the model to the extinctions; 1 and 2 to scale[v][m] * exp(-p), then
+    p = log(scale / value).  scale: the photon count (1) or count x mean energy (2)."""
+    p = np.array(extinction, dtype=np.float32, copy=True)
+    if domain == 0:
+        return saturation_value(p, kind, a, b, soft_a, soft_b)
+    s = np.asarray(scale, np.float32).reshape(p.shape[:2] + (1,) * (p.ndim - 2))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        x = saturation_value((s * np.exp(-p)).astype(np.float32), kind, a, b, soft_a, soft_b)
+        return np.log((s / x).astype(np.float32)).astype(np.float32)
