@@ -210,13 +210,18 @@ class SpectralEffectsExtension:
       photons_per_pixel [bins][modules] or None: the nested PoissonNoiseExtension's i0 in
                                    each bin (photonsPerPixel with the bin's flux); None for
                                    the linear case
-      fixed_seed:                  the nested noise extension's fixed seed (None: random)"""
+      fixed_seed:                  the nested noise extension's fixed seed (None: random)
+
+    Material volumes given as VoxelVolumes are uploaded on first use and stay resident
+    while the same objects are projected again (they must not be modified in between;
+    pass resident Volumes to manage that explicitly); release() frees them."""
 
     def __init__(self, ctx: Context, settings: Optional[Settings] = None):
         self.ctx = ctx
         self.settings = settings or Settings()
         self._pm = None
         self._calls = 0
+        self._resident = []
 
     def configure(self, pmats, channels: int, rows: int, mu_per_mm, intensities, total_intensity,
                   response=None, photons_per_pixel=None, fixed_seed: Optional[int] = None) -> None:
@@ -256,7 +261,11 @@ class SpectralEffectsExtension:
             raise ValueError("one mass attenuation column per material")
         P = self._pm if hasattr(self._pm, "is_cuda") else torch.from_numpy(np.ascontiguousarray(self._pm)).cuda()
         V, Mod = int(P.shape[0]), int(P.shape[1])
-        vols = [self.ctx.volume(v, self.settings.storage) for v in material_densities]
+        # the material volumes stay resident while the same objects are projected again
+        if len(self._resident) != M:
+            self.release()
+            self._resident = [_Resident(self.ctx) for _ in range(M)]
+        vols = [r.get(v, self.settings.storage) for r, v in zip(self._resident, material_densities)]
         try:
             projs = torch.empty((M, V, Mod, R, C_), dtype=torch.float32, device="cuda")
             self.ctx.project_batch([(vol, P, projs[m]) for m, vol in enumerate(vols)], self.settings)
@@ -285,8 +294,12 @@ class SpectralEffectsExtension:
             return out
         finally:
             torch.cuda.synchronize()
-            for vol in vols:
-                vol.release()
+
+    def release(self) -> None:
+        """Free the resident material volumes."""
+        for r in getattr(self, "_resident", []):
+            r.release()
+        self._resident = []
 
 
 class PoissonNoiseExtension:

@@ -248,6 +248,11 @@ def test_noisy_spectral_extension_matches_the_oracle_draw_for_draw(ctx):
     np.testing.assert_array_equal(ext2.project([VoxelVolume(water, vox), VoxelVolume(bone, vox)]).cpu().numpy(),
                                   got)
     torch.cuda.synchronize()
+    # the material volumes stayed resident across calls; release() frees them
+    used = ctx.memory_used()
+    ext.release()
+    ext2.release()
+    assert ctx.memory_used() < used
 
 
 # ---- dynamic volumes ------------------------------------------------------------------------
