@@ -147,8 +147,10 @@ class DynamicProjectorExtension:
     """DynamicProjectorExtension (projectors/dynamicprojectorextension.cpp:37-60) around the
     B200 projector.  The reference re-projects every view with the volume set to that
     view's time.  For a LinearDynamicVolume the projection is linear in the voxels, so
-    all views come from two batched projections (slope and offset volumes) and one
-    combine launch; any other volume is projected as it is."""
+    all views come from one batched projection of the slope and offset volumes and one
+    combine launch; any other volume is projected as it is.  The volumes are uploaded on
+    first use and stay resident while the same objects are projected again (they must
+    not be modified in between); release() frees them."""
 
     def __init__(self, ctx: Context, settings: Optional[Settings] = None):
         self.ctx = ctx
@@ -156,6 +158,7 @@ class DynamicProjectorExtension:
         self._pm = None
         self._dims = None
         self._times = None
+        self._resident = [_Resident(ctx), _Resident(ctx)]
 
     def configure(self, pmats, channels: int, rows: int, time_stamps: Sequence[float]) -> None:
         """pmats (views, modules, 3, 4) (host or device); time_stamps: one per view in
@@ -173,22 +176,20 @@ class DynamicProjectorExtension:
         C_, R = self._dims
         P = self._pm if hasattr(self._pm, "is_cuda") else torch.from_numpy(np.ascontiguousarray(self._pm)).cuda()
         if not isinstance(volume, LinearDynamicVolume):
-            vol = self.ctx.volume(volume, self.settings.storage)
-            try:
-                return self.ctx.project(vol, P, C_, R, self.settings)
-            finally:
-                torch.cuda.synchronize()
-                vol.release()
-        vs = self.ctx.volume(volume.slope, self.settings.storage)
-        vo = self.ctx.volume(volume.offset, self.settings.storage)
-        try:
-            ps = self.ctx.project(vs, P, C_, R, self.settings)
-            po = self.ctx.project(vo, P, C_, R, self.settings)
-            return self.ctx.combine_linear(ps, po, self._times, torch.empty_like(ps))
-        finally:
-            torch.cuda.synchronize()
-            vs.release()
-            vo.release()
+            return self.ctx.project(self._resident[0].get(volume, self.settings.storage), P, C_, R, self.settings)
+        vs = self._resident[0].get(volume.slope, self.settings.storage)
+        vo = self._resident[1].get(volume.offset, self.settings.storage)
+        V, M = int(P.shape[0]), int(P.shape[1])
+        both = torch.empty((2, V, M, R, C_), dtype=torch.float32, device="cuda")
+        self.ctx.project_batch([(vs, P, both[0]), (vo, P, both[1])], self.settings)
+        out = self.ctx.combine_linear(both[0], both[1], self._times, torch.empty_like(both[0]))
+        torch.cuda.synchronize()
+        return out
+
+    def release(self) -> None:
+        """Free the resident volumes."""
+        for r in self._resident:
+            r.release()
 
 
 class SpectralEffectsExtension:
