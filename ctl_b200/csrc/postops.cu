@@ -283,7 +283,15 @@ __global__ void saturation_kernel(float* __restrict__ data, uint32_t n_views, ui
 // the intensity domain as spectral_kernel does.  `quiet[b]`: the bin's i0 sums
 // to zero, and the nested noise step leaves its projections as they are
 // (poissonnoiseextension.cpp:160).
-__global__ void spectral_noisy_kernel(const float* __restrict__ proj, uint32_t n_materials, uint32_t n_views,
+// Register budget of the (bin, material) noise kernel: sized for 3 resident 256-thread
+// blocks per SM (75 registers, no spills).  Unbounded it took 90 registers and 2 blocks,
+// and ran 12% slower (286 vs 252 ms at 360 x 512^2, 30 bins, 2 materials); 4 blocks
+// (64 registers, a small spill) were no faster than 3.
+#ifndef CTLCU_NOISE_MINB
+#define CTLCU_NOISE_MINB 3
+#endif
+__global__ void __launch_bounds__(256, CTLCU_NOISE_MINB)
+    spectral_noisy_kernel(const float* __restrict__ proj, uint32_t n_materials, uint32_t n_views,
                                       uint32_t n_modules, uint32_t ppm, const float* __restrict__ mu,
                                       const double* __restrict__ intensity, const float* __restrict__ response,
                                       const int* __restrict__ skip, const int* __restrict__ quiet, uint32_t n_bins,
