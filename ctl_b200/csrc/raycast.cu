@@ -570,39 +570,48 @@ __global__ void __maxnreg__(CTLCU_CELL_MAXREG) cells_kernel(const ProjectArgs a)
 // until all requests' items are done.  Work items of one request are its
 // blocks in the order of the single-request launch, so blocks running at the
 // same time work on neighbouring views of one volume.
+//
+// Per item the block's bookkeeping stays off the critical path: thread 0 takes the
+// index of its next item from the counter while the current one runs; a block's
+// items only grow, so the request of an item is found by scanning forward from the
+// previous one; and the request's launch arguments are copied to shared memory
+// only when the request changes.
 template <Mode M, Accum ACC, int U>
 __global__ void __maxnreg__(CTLCU_CELL_MAXREG)
     batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter)
 {
     __shared__ ProjectArgs sa;
-    __shared__ uint32_t s_item, s_local;
+    __shared__ uint32_t s_req, s_local;
     static_assert(sizeof(ProjectArgs) % 4 == 0, "word copy");
+    uint32_t next = 0, req = 0;  // thread 0: the item to run next and the request of the last one
+    if (threadIdx.x == 0)
+        next = atomicAdd(counter, 1u);
+    uint32_t loaded = 0xffffffffu;  // request whose arguments `sa` holds (the same in every thread)
     for (;;) {
         if (threadIdx.x == 0) {
-            const uint32_t it = atomicAdd(counter, 1u);
-            uint32_t lo = 0;
+            const uint32_t it = next;
             if (it < total) {
-                uint32_t hi = n_reqs - 1;  // last request with first_item <= it
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi + 1) / 2;
-                    if (reqs[mid].first_item <= it)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                s_local = it - reqs[lo].first_item;
+                while (req + 1 < n_reqs && reqs[req + 1].first_item <= it)
+                    ++req;  // the last request with first_item <= it
+                s_local = it - reqs[req].first_item;
+                s_req = req;
+                next = atomicAdd(counter, 1u);
+            } else {
+                s_req = 0xffffffffu;
             }
-            s_item = it < total ? lo : 0xffffffffu;
         }
         __syncthreads();
-        const uint32_t r = s_item;
+        const uint32_t r = s_req;
         if (r == 0xffffffffu)
             return;
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&reqs[r].a);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
-        for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
-            dst[i] = src[i];
-        __syncthreads();
+        if (r != loaded) {  // uniform: every thread read the same s_req
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&reqs[r].a);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+            for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
+                dst[i] = src[i];
+            loaded = r;
+            __syncthreads();
+        }
         cells_item<M, ACC, U>(sa, s_local, threadIdx.x);
         __syncthreads();
     }
