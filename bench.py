@@ -826,12 +826,21 @@ def run_c5(args):
     vols = [ctx.volume(VoxelVolume(v, (1.0, 1.0, 1.0)), L.BF16) for v in W.c5_volumes()]
     kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
                                  "pairs": L.KERNEL_PAIRS}[args.kernel]
-    server = DRRServer(ctx, vols, 256, 256, Settings(kernel=kernel), streams=3, max_batch=256,
-                       budget_bytes=40 * 10**9)
+    # 2 streams and batches of at most 24 views: a batch's persistent launch holds the SMs
+    # until it is done, so bounding its views bounds how long later requests wait behind it
+    # (a sweep of 1-3 streams and 24-256-view caps gave the lowest p99 at 500-1300 req/s
+    # for this setting, at the same capacity)
+    server = DRRServer(ctx, vols, 256, 256, Settings(kernel=kernel), streams=2, max_batch=256,
+                       budget_bytes=40 * 10**9, max_batch_views=24)
     base = W.c5_base_view()
     server.warm_up(typical_pmats=np.repeat(base[None], 8, axis=0) if kernel == L.KERNEL_AUTO else None)
-    # capacity: all requests offered at once
-    cap = server.run(poisson_requests(1e7, 2000, len(vols), base, seed=50)).summary()
+    # capacity: all requests offered at once.  The first run of this size also grows the
+    # device allocators (outputs and batch descriptors of 2000 requests) and ran up to 30%
+    # slower, so one untimed run comes first; then three runs, the median reported with the spread
+    server.run(poisson_requests(1e7, 2000, len(vols), base, seed=49))
+    caps = [server.run(poisson_requests(1e7, 2000, len(vols), base, seed=50 + 100 * i)).summary() for i in range(3)]
+    caps.sort(key=lambda c: c["throughput_req_s"])
+    cap = dict(caps[1], runs_req_s=[c["throughput_req_s"] for c in caps])
     rate = 2000.0
     n = int(rate * args.serve_seconds)
     at = server.run(poisson_requests(rate, n, len(vols), base, seed=51)).summary()

@@ -73,7 +73,8 @@ class ServeStats:
 class DRRServer:
     def __init__(self, ctx: Context, volumes: Sequence[Volume], channels: int, rows: int,
                  settings: Optional[Settings] = None, streams: int = 2, max_batch: int = 256,
-                 budget_bytes: int = 40 * 10**9, refuse: bool = False, deadline_ms: Optional[float] = None):
+                 budget_bytes: int = 40 * 10**9, refuse: bool = False, deadline_ms: Optional[float] = None,
+                 max_batch_views: Optional[int] = None):
         import torch
         self.torch = torch
         self.ctx = ctx
@@ -82,6 +83,10 @@ class DRRServer:
         self.settings = settings or Settings()
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.max_batch = max_batch
+        # a batch stops taking requests once it holds this many views (the first request
+        # always goes in).  A batch's persistent launch holds the SMs until it is done, so
+        # batches on other streams wait behind it; bounding its views bounds that wait.
+        self.max_batch_views = max_batch_views
         self.refuse = refuse
         # a queued request that has waited longer than this when a stream frees is
         # refused rather than served late
@@ -174,7 +179,15 @@ class DRRServer:
                             kept.append(r)
                     queue = kept
                 if inflight[i] is None and queue:
-                    batch, queue = queue[: self.max_batch], queue[self.max_batch:]
+                    take = min(self.max_batch, len(queue))
+                    if self.max_batch_views is not None:
+                        views, take = 0, 0
+                        while take < min(self.max_batch, len(queue)):
+                            views += int(queue[take].pmats.shape[0])
+                            if take > 0 and views > self.max_batch_views:
+                                break
+                            take += 1
+                    batch, queue = queue[:take], queue[take:]
                     with torch.cuda.stream(s):
                         # one host-to-device copy for the whole batch's matrices
                         allP = torch.from_numpy(np.concatenate([r.pmats.reshape(-1, 12) for r in batch]))

@@ -47,6 +47,27 @@ def test_server_results_equal_alone_and_oracle():
     ctx.close()
 
 
+def test_server_view_cap_bounds_every_batch():
+    """With max_batch_views, a batch takes requests until the next would pass the cap (the
+    first always goes in); every request is served, with its single-call result."""
+    from ctl_b200 import _lib as L
+    ctx = Context(0)
+    vol = Ph.ellipsoid_phantom((32, 32, 32), (3, 3, 3), 4, seed=9)
+    h = ctx.volume(VoxelVolume(vol, (3, 3, 3)), L.BF16)
+    server = DRRServer(ctx, [h], 48, 40, Settings(), streams=1, max_batch=64, max_batch_views=7)
+    server.warm_up()
+    reqs = poisson_requests(1e7, 40, 1, _base_view(), seed=11, views=(1, 9))   # all queued at once
+    stats = server.run(reqs)
+    assert stats.completed == 40 and stats.refused == 0
+    total_views = sum(int(r.pmats.shape[0]) for r in reqs)
+    assert stats.batches >= total_views / 9   # no batch beyond 7 views unless one request alone has more
+    for r in reqs[::7]:
+        alone = ctx.project(h, r.pmats, 48, 40, Settings())
+        np.testing.assert_allclose(r.out.cpu().numpy(), alone, rtol=1e-6, atol=1e-7)
+    h.release()
+    ctx.close()
+
+
 def test_server_admission_by_budget():
     from ctl_b200 import _lib as L
     ctx = Context(0)
