@@ -334,6 +334,19 @@ def run_ours(args):
                 line["cpu_baseline"] = {"value": rate, "unit": "projections/s", "cores": os.cpu_count(),
                                         "kind": "reference",
                                         "sample": f"{n} of {N_VIEWS} views evenly spaced, {dt:.1f} s"}
+            # the FP64 formulation of the reference's CPU projector (RayCasterProjectorCPU,
+            # raycasterprojectorcpu.cpp:132-285), as the oracle restates it, timed once beside it
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            oracle.project_fp64(vol, VOXEL, P[:1], CHANNELS, ROWS, threads=threads)
+            t1 = time.perf_counter() - t0
+            n = int(max(1, min(N_VIEWS, round(0.5 * args.cpu_seconds / max(t1, 1e-3)))))
+            idx = np.linspace(0, N_VIEWS - 1, n).round().astype(int)
+            t0 = time.perf_counter()
+            oracle.project_fp64(vol, VOXEL, P[idx], CHANNELS, ROWS, threads=threads)
+            dt = time.perf_counter() - t0
+            line["cpu_fp64_twin"] = {"value": n / dt, "unit": "projections/s", "cores": threads, "kind": "port",
+                                     "sample": f"{n} of {N_VIEWS} views evenly spaced, {dt:.1f} s"}
         print(json.dumps(line))
     volume.release()
     ctx.close()
