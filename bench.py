@@ -324,7 +324,11 @@ def run_ours(args):
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch"
                                            if traffic else "not captured for this variant",
                          "peak_source": f"{sms} SMs x 128 B/clk x {mhz:.0f} MHz sampled SM clock",
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         # the DRAM side: the captured traffic over this run's launch time, against
+                         # the measured HBM copy rate (the bound that does not bind this kernel)
+                         "dram_gb_s": traffic / (kernel_ms / 1e3) / 1e9 if traffic else None,
+                         "dram_frac_of_hbm": traffic / (kernel_ms / 1e3) / 1e9 / hbm_peak() if traffic else None},
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu_baseline:
