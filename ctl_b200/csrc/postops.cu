@@ -1,5 +1,7 @@
-// Post-projection operations on the device: extinction <-> intensity and
-// Poisson (quantum) noise.
+// Post-projection operations on the device: extinction <-> intensity, Poisson
+// (quantum) noise, detector saturation, and the per-pixel combines of the
+// projector extensions (focal-spot average, linear dynamic volumes, spectral
+// effects with and without nested noise).
 //
 // Reference (modules/src/...):
 //   SingleViewData::transformToExtinction / transformToCounts (img/singleviewdata.cpp:135-172):
