@@ -269,7 +269,9 @@ def run_ours(args):
     h_P = torch.from_numpy(P).pin_memory()
     h_out = torch.empty((n_views, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
     desc_vol = VoxelVolume(h_vol.numpy(), VOXEL)
-    for _ in range(max(1, args.warmup // 2)):
+    # as many warm-up calls as device steps: with one, the first timed calls still ran
+    # up to 8% slower and the end-to-end number varied from run to run
+    for _ in range(max(1, args.warmup)):
         ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
     barrier(world)
     e2e_ms = []
@@ -898,7 +900,7 @@ def main():
     ap.add_argument("--unroll", type=int, default=0, choices=[0, 2, 4, 8])
     ap.add_argument("--views", type=int, default=N_VIEWS,
                     help="views per step (360 = the configuration; fewer = a small profiling case)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
