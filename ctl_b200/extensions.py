@@ -45,23 +45,24 @@ class _Resident:
     def __init__(self, ctx: Context):
         self.ctx = ctx
         self._key = None
+        self._data = None  # the uploaded array, held so that its id stays unique while cached
         self._vol: Optional[Volume] = None
 
     def get(self, volume, storage: int) -> Volume:
         if isinstance(volume, Volume):
             return volume
         key = (id(volume.data), tuple(volume.data.shape), tuple(volume.voxel_size), tuple(volume.offset), storage)
-        if key != self._key:
+        if key != self._key or self._data is not volume.data:
             if self._vol is not None:
                 self._vol.release()
             self._vol = self.ctx.volume(volume, storage)
-            self._key = key
+            self._key, self._data = key, volume.data
         return self._vol
 
     def release(self):
         if self._vol is not None:
             self._vol.release()
-        self._vol, self._key = None, None
+        self._vol, self._key, self._data = None, None, None
 
 
 class ArealFocalSpotExtension:

@@ -21,6 +21,40 @@ def test_discretization_grid_matches_the_oracle_restatement():
     assert discretization_grid(2, 2) == [(-0.5, -0.5), (-0.5, 0.5), (0.5, -0.5), (0.5, 0.5)]
 
 
+def test_resident_volume_is_uploaded_once_per_array():
+    """The extensions' volume cache: one upload while the same array is projected again,
+    a new upload (and the old one released) for another array, voxel size or storage."""
+    from ctl_b200.extensions import _Resident
+    from ctl_b200.projector import VoxelVolume
+
+    class _Vol:
+        released = False
+
+        def release(self):
+            self.released = True
+
+    class _Ctx:
+        uploads = 0
+
+        def volume(self, vol, storage):
+            self.uploads += 1
+            return _Vol()
+
+    ctx = _Ctx()
+    cache = _Resident(ctx)
+    a = np.zeros((4, 5, 6), np.float32)
+    first = cache.get(VoxelVolume(a, (1.0, 1.0, 1.0)), 0)
+    assert cache.get(VoxelVolume(a, (1.0, 1.0, 1.0)), 0) is first and ctx.uploads == 1
+    b = np.zeros((4, 5, 6), np.float32)
+    second = cache.get(VoxelVolume(b, (1.0, 1.0, 1.0)), 0)
+    assert ctx.uploads == 2 and first.released and second is not first
+    cache.get(VoxelVolume(b, (2.0, 1.0, 1.0)), 0)
+    cache.get(VoxelVolume(b, (2.0, 1.0, 1.0)), 1)
+    assert ctx.uploads == 4
+    cache.release()
+    assert cache.get(VoxelVolume(b, (2.0, 1.0, 1.0)), 1) is not None and ctx.uploads == 5
+
+
 def test_oracle_source_shift_moves_the_decomposed_source():
     """The source that the reference's decomposition recovers from a shifted
     matrix is the gantry's source moved by sourceRotation * shift."""
