@@ -218,6 +218,28 @@ def _noisy_spectral_composition(projs, mu, inten, response, total, i0, seed):
     return np.log(total.astype(np.float32)[:, None, None, None] / acc), call
 
 
+def test_spectral_configure_checks_its_inputs_and_counts_nested_calls():
+    """configure() rejects inputs of the wrong shapes; the nested projections per call are
+    materials x bins with intensity (a bin without intensity makes no call)."""
+    from ctl_b200.extensions import SpectralEffectsExtension
+    from ctl_b200.projector import Context
+    ext = SpectralEffectsExtension(Context.__new__(Context))   # type only: no device is touched
+    P = np.zeros((5, 2, 3, 4))
+    mu = np.ones((4, 3), np.float32)
+    inten = np.ones((4, 5))
+    inten[1] = 0.0
+    ext.configure(P, 8, 6, mu, inten, inten.sum(0))
+    assert ext.is_linear() and ext.nested_calls() == 3 * 3
+    ext.configure(P, 8, 6, mu, inten, inten.sum(0), photons_per_pixel=np.ones((4, 2)), fixed_seed=1)
+    assert not ext.is_linear()
+    for bad in (dict(intensities=np.ones((4, 4))), dict(total_intensity=np.ones(4)),
+                dict(response=np.ones(3)), dict(photons_per_pixel=np.ones((4, 3)))):
+        args = dict(mu_per_mm=mu, intensities=inten, total_intensity=inten.sum(0))
+        args.update(bad)
+        with pytest.raises(ValueError):
+            ext.configure(P, 8, 6, **args)
+
+
 def test_noisy_spectral_composition_tends_to_the_linear_case():
     """With very many photons the noisy loop approaches the linear formula, a bin
     without photons passes without noise, and the call count covers the live bins."""

@@ -39,6 +39,31 @@ def test_count_domain_round_trip_without_saturation():
     np.testing.assert_allclose(out, p, atol=2e-6)
 
 
+def test_extension_scale_per_domain():
+    """The [view][module] scale the extension hands to the device step: nothing in the
+    extinction domain, the photon count, or count x the view's mean energy in FP32."""
+    from ctl_b200 import _lib as L
+    from ctl_b200.extensions import DetectorSaturationExtension, linear_saturation
+    from ctl_b200.projector import Context
+
+    class _Nested:
+        ctx = Context.__new__(Context)   # type only: no device is touched here
+
+    m = linear_saturation(0.0, 1.0)
+    assert DetectorSaturationExtension(_Nested(), m, L.SATURATION_EXTINCTION).scale(3, 2) is None
+    n0 = [1e4, 2e4]
+    count = DetectorSaturationExtension(_Nested(), m, L.SATURATION_PHOTON_COUNT, photons_per_pixel=n0).scale(3, 2)
+    np.testing.assert_array_equal(count, np.array([n0] * 3, np.float32))
+    e = [50.0, 60.0, 70.0]
+    inten = DetectorSaturationExtension(_Nested(), m, L.SATURATION_INTENSITY, photons_per_pixel=n0,
+                                        mean_energy=e).scale(3, 2)
+    np.testing.assert_array_equal(inten, (np.array([n0] * 3, np.float32) * np.float32(e)[:, None]))
+    with pytest.raises(ValueError):
+        DetectorSaturationExtension(_Nested(), m, L.SATURATION_PHOTON_COUNT)
+    with pytest.raises(TypeError):
+        DetectorSaturationExtension(object(), m, L.SATURATION_EXTINCTION)
+
+
 # ---- device ----------------------------------------------------------------------------------
 
 @pytest.fixture(scope="module")
