@@ -74,6 +74,29 @@ def test_unrolls_agree_and_stay_within_the_oracle_bound(kernel, unroll):
         h.release()
 
 
+@pytest.mark.parametrize("storage", [L.F32, L.BF16, L.F16])
+def test_shapes_with_16bit_storage_nearest_upsampling_and_texture(storage):
+    """Every sample loop shares the pixel mapping: non-default shapes give the default
+    shape's bits for 16-bit storage, the nearest-voxel loop, up-sampled volumes and the
+    texture filter too."""
+    vol, P = _job()
+    C, R = 37, 29
+    forms = [Settings(), Settings(interpolate=False), Settings(volume_upsampling=2),
+             Settings(interp_mode=L.INTERP_TEXTURE)]
+    with Context(0) as ctx:
+        h = ctx.volume(VoxelVolume(vol, (2.0, 2.0, 2.0)), storage)
+        for s in forms:
+            if storage == L.BF16 and s.interp_mode == L.INTERP_TEXTURE:
+                continue   # texture filtering takes F32 and F16 storage only (no BF16 texture format)
+            base = ctx.project(h, P, C, R, s)
+            for b, v, lx in [(128, 4, 8), (512, 1, 4), (256, 4, 4)]:
+                s2 = Settings(interpolate=s.interpolate, volume_upsampling=s.volume_upsampling,
+                              interp_mode=s.interp_mode, block_rays=b, views_per_block=v, lanes_x=lx)
+                np.testing.assert_array_equal(ctx.project(h, P, C, R, s2), base,
+                                              err_msg=f"{s} with shape {b} rays / {v} views / lanes {lx}")
+        h.release()
+
+
 def test_multimodule_shapes_with_subrays():
     vol, P = _multimodule()
     C, R = 12, 10
