@@ -156,6 +156,35 @@ def test_autotuned_shape_serves_later_calls():
         h.release()
 
 
+def test_plans_and_the_noalloc_call_run_the_given_shape():
+    """A CUDA-graph plan (launched twice) and the no-allocation call, with a non-default
+    shape, give the single call's bits with that shape."""
+    import torch
+    vol, P = _job()
+    C, R = 37, 29
+    with Context(0) as ctx:
+        h = ctx.volume(VoxelVolume(vol, (2.0, 2.0, 2.0)))
+        s = Settings(block_rays=128, views_per_block=4, lanes_x=8, unroll=8)
+        alone = ctx.project(h, P, C, R, s)
+        dP = torch.from_numpy(P).cuda()
+        out = torch.zeros((P.shape[0], 1, R, C), device="cuda")
+        torch.cuda.synchronize()
+        plan = ctx.plan([(h, dP, out)], s)
+        for _ in range(2):
+            plan.launch()
+            ctx.sync()
+            np.testing.assert_array_equal(out.cpu().numpy(), alone)
+            out.zero_()
+            torch.cuda.synchronize()
+        plan.close()
+        out2 = torch.zeros_like(out)
+        torch.cuda.synchronize()
+        ctx.project_noalloc(h, dP, out2, s)
+        ctx.sync()
+        np.testing.assert_array_equal(out2.cpu().numpy(), alone)
+        h.release()
+
+
 def test_batch_runs_the_given_shape():
     import torch
     vol, P = _job()
