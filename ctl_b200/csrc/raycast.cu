@@ -184,14 +184,22 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v,
 __device__ __forceinline__ int floor_div(int i, int f) { return i >= 0 ? i / f : -((f - 1 - i) / f); }
 
 // Sample loop, trilinear with zero border, volume stored as T (padded).
+// Positions are formed relative to the integer part (ox, oy, oz) of the first
+// sample, for the reason given at CellFrame; the offset is folded into the
+// ray's base pointer and its clamp bounds, so a sample costs what it did with
+// absolute coordinates.
 template <typename T, Accum ACC, bool UP>
 __device__ __forceinline__ void march_trilinear(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
     const T* __restrict__ vol = static_cast<const T*>(a.vol);
     const int sy = a.sy, sz = a.sz;
     const int mx = a.ext[0] - 2, my = a.ext[1] - 2, mz = a.ext[2] - 2;
-    const float bx = (float)r.base[0], by = (float)r.base[1], bz = (float)r.base[2];
+    const int ox = (int)rint(r.base[0]), oy = (int)rint(r.base[1]), oz = (int)rint(r.base[2]);
+    const float bx = (float)(r.base[0] - ox), by = (float)(r.base[1] - oy), bz = (float)(r.base[2] - oz);
     const float dx = (float)r.step[0], dy = (float)r.step[1], dz = (float)r.step[2];
+    // the ray's origin tap; indexes relative to it are clamped so that the
+    // absolute tap stays in [0, m] on each axis
+    const T* __restrict__ vray = vol + ((ptrdiff_t)ox + (ptrdiff_t)oy * sy + (ptrdiff_t)oz * sz);
     for (int k = 0; k < r.n; ++k) {
         const float kf = static_cast<float>(k);
         const float ux = fmaf(kf, dx, bx);
@@ -201,10 +209,10 @@ __device__ __forceinline__ void march_trilinear(const ProjectArgs& a, const Ray&
         const float wx = ux - fx, wy = uy - fy, wz = uz - fz;
         float v000, v100, v010, v110, v001, v101, v011, v111;
         if (!UP) {
-            const int ix = clampi(__float2int_rz(fx), 0, mx);
-            const int iy = clampi(__float2int_rz(fy), 0, my);
-            const int iz = clampi(__float2int_rz(fz), 0, mz);
-            const T* p = vol + (ix + iy * sy + iz * sz);
+            const int ix = clampi(__float2int_rz(fx), -ox, mx - ox);
+            const int iy = clampi(__float2int_rz(fy), -oy, my - oy);
+            const int iz = clampi(__float2int_rz(fz), -oz, mz - oz);
+            const T* p = vray + (ix + iy * sy + iz * sz);
             v000 = load_voxel(p);
             v100 = load_voxel(p + 1);
             v010 = load_voxel(p + sy);
@@ -216,9 +224,9 @@ __device__ __forceinline__ void march_trilinear(const ProjectArgs& a, const Ray&
         } else {
             // virtual replication: grid index g maps to stored voxel floor(g / f)
             const int f = a.up;
-            const int gx = __float2int_rz(fmaxf(fminf(fx, 1.0e8f), -1.0e8f));
-            const int gy = __float2int_rz(fmaxf(fminf(fy, 1.0e8f), -1.0e8f));
-            const int gz = __float2int_rz(fmaxf(fminf(fz, 1.0e8f), -1.0e8f));
+            const int gx = __float2int_rz(fmaxf(fminf(fx, 1.0e8f), -1.0e8f)) + ox;
+            const int gy = __float2int_rz(fmaxf(fminf(fy, 1.0e8f), -1.0e8f)) + oy;
+            const int gz = __float2int_rz(fmaxf(fminf(fz, 1.0e8f), -1.0e8f)) + oz;
             const int x0 = clampi(floor_div(gx, f) + kPad, 0, mx + 1);
             const int x1 = clampi(floor_div(gx + 1, f) + kPad, 0, mx + 1);
             const int y0 = clampi(floor_div(gy, f) + kPad, 0, my + 1) * sy;
@@ -262,10 +270,37 @@ __device__ __forceinline__ void march_nearest(const ProjectArgs& a, const Ray& r
     }
 }
 
+// Per-ray frame of the cell and pair loops.  Each axis of the first-sample
+// position is split into an integer I = rint(base) and an FP32 remainder, and
+// positions are formed as v' = (base - I) + k step.  Along an axis on which the
+// ray moves little (a ray grazing a face of the volume) v' stays near zero,
+// where FP32 is fine-grained; an absolute coordinate of a few hundred voxels
+// would carry a rounding offset of up to 3e-5 voxel into every sample, and on
+// a grazing ray that offset changes the line integral by up to 1e-3.  I is
+// folded into the rounding constant m = kMagic + I (exact in FP32, |I| < 2^22),
+// so t = v' + m has the bits kMagicBits + I + rint(v') of the absolute cell.
+struct CellFrame {
+    float2 bxy;  // base - I, x and y
+    float bz;
+    float2 mxy;  // kMagic + I, x and y
+    float mz;
+};
+
+__device__ __forceinline__ CellFrame cell_frame(const Ray& r)
+{
+    CellFrame f;
+    const double ix = rint(r.base[0]), iy = rint(r.base[1]), iz = rint(r.base[2]);
+    f.bxy = make_float2((float)(r.base[0] - ix), (float)(r.base[1] - iy));
+    f.bz = (float)(r.base[2] - iz);
+    f.mxy = make_float2(__fadd_rn(kMagic, (float)ix), __fadd_rn(kMagic, (float)iy));
+    f.mz = __fadd_rn(kMagic, (float)iz);
+    return f;
+}
+
 // One sample from the coefficient cells at step kk (both lanes of kk hold k).
-// Per axis: v = base + k step; t = v + kMagic rounds v to the cell index
-// (its bits minus kMagicBits); h = v - (t - kMagic) is the offset from the
-// cell centre in [-1/2, 1/2].  x and y go through packed f32x2 arithmetic.
+// Per axis: v' = (base - I) + k step; t = v' + m rounds to the cell index (its
+// bits minus kMagicBits, see CellFrame); h = v' - (t - m) is the offset from
+// the cell centre in [-1/2, 1/2].  x and y go through packed f32x2 arithmetic.
 // A sample that lands exactly between two cells may take either of them; both
 // give the same interpolated value.  The cell index is clamped to the array as
 // a guard; the loop bounds already keep every sample inside it.
@@ -277,30 +312,27 @@ struct CellCache {
 #if CTLCU_CELL_PREFETCH > 0
 // Cell index of the sample at step kk (the cell layout makes the magic
 // offsets cancel, see CellLayout), clamped to the array.
-__device__ __forceinline__ uint32_t cell_index(float2 kk, float2 bxy, float bz, float2 dxy, float dz,
+__device__ __forceinline__ uint32_t cell_index(float2 kk, const CellFrame& fr, float2 dxy, float dz,
                                                uint32_t sy, uint32_t sz, uint32_t cmax)
 {
-    const float2 txy = __fadd2_rn(__ffma2_rn(kk, dxy, bxy), make_float2(kMagic, kMagic));
-    const float tz = __fadd_rn(fmaf(kk.x, dz, bz), kMagic);
+    const float2 txy = __fadd2_rn(__ffma2_rn(kk, dxy, fr.bxy), fr.mxy);
+    const float tz = __fadd_rn(fmaf(kk.x, dz, fr.bz), fr.mz);
     const uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
     return min(idx, cmax);
 }
 #endif
 
 __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const char* __restrict__ cells, float2 kk,
-                                             float2 bxy,
-                                             float bz, float2 dxy, float dz, uint32_t sy, uint32_t sz,
+                                             const CellFrame& fr, float2 dxy, float dz, uint32_t sy, uint32_t sz,
                                              uint32_t cmax, CellCache& cc)
 {
-    const float2 magic2 = make_float2(kMagic, kMagic);
-    const float2 nmagic2 = make_float2(-kMagic, -kMagic);
     const float2 none2 = make_float2(-1.0f, -1.0f);
-    const float2 vxy = __ffma2_rn(kk, dxy, bxy);
-    const float vz = fmaf(kk.x, dz, bz);
-    const float2 txy = __fadd2_rn(vxy, magic2);
-    const float tz = __fadd_rn(vz, kMagic);
-    const float2 fxy = __fadd2_rn(txy, nmagic2);
-    const float fz = __fadd_rn(tz, -kMagic);
+    const float2 vxy = __ffma2_rn(kk, dxy, fr.bxy);
+    const float vz = fmaf(kk.x, dz, fr.bz);
+    const float2 txy = __fadd2_rn(vxy, fr.mxy);
+    const float tz = __fadd_rn(vz, fr.mz);
+    const float2 fxy = __ffma2_rn(fr.mxy, none2, txy);  // t - m, exact
+    const float fz = __fsub_rn(tz, fr.mz);
     const float2 hxy = __ffma2_rn(fxy, none2, vxy);
     const float hz = fmaf(fz, -1.0f, vz);
     uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
@@ -358,8 +390,7 @@ template <Accum ACC, int U>
 __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
     const char* __restrict__ cells = static_cast<const char*>(a.cells);
-    const float2 bxy = make_float2((float)r.base[0], (float)r.base[1]);
-    const float bz = (float)r.base[2];
+    const CellFrame fr = cell_frame(r);
     const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
     const float dz = (float)r.step[2];
     const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
@@ -378,20 +409,20 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
             // pull the cell of sample k + PREFETCH into L1 without waiting for it:
             // an asynchronous 4-byte copy into a scratch shared word that is never read
             const float ahead = (float)CTLCU_CELL_PREFETCH;
-            const uint32_t pi = cell_index(__fadd2_rn(kk, make_float2(ahead, ahead)), bxy, bz, dxy, dz, sy, sz, cmax);
+            const uint32_t pi = cell_index(__fadd2_rn(kk, make_float2(ahead, ahead)), fr, dxy, dz, sy, sz, cmax);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(prefetch_slot),
                          "l"(cells + (size_t)pi * kCellBytes));
         }
 #endif
 #pragma unroll
         for (int j = 0; j < U; ++j) {
-            part += cell_sample(a.cell_tex, cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc);
+            part += cell_sample(a.cell_tex, cells, kk, fr, dxy, dz, sy, sz, cmax, cc);
             kk = __fadd2_rn(kk, one2);
         }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(cell_sample(a.cell_tex, cells, kk, bxy, bz, dxy, dz, sy, sz, cmax, cc));
+        acc.add(cell_sample(a.cell_tex, cells, kk, fr, dxy, dz, sy, sz, cmax, cc));
         kk = __fadd2_rn(kk, one2);
     }
 #if CTLCU_CELL_PREFETCH > 0
@@ -408,19 +439,17 @@ struct PairCache {
 // One sample from the x-pair array: the same cell index and centre offsets as
 // cell_sample, four 8-byte entries loaded only when the cell changes, x by
 // mid + hx diff, then y and z linearly.
-__device__ __forceinline__ float pair_sample(const char* __restrict__ pairs, float2 kk, float2 bxy, float bz,
+__device__ __forceinline__ float pair_sample(const char* __restrict__ pairs, float2 kk, const CellFrame& fr,
                                              float2 dxy, float dz, uint32_t sy, uint32_t sz, uint32_t pmax,
                                              PairCache& pc)
 {
-    const float2 magic2 = make_float2(kMagic, kMagic);
-    const float2 nmagic2 = make_float2(-kMagic, -kMagic);
     const float2 none2 = make_float2(-1.0f, -1.0f);
-    const float2 vxy = __ffma2_rn(kk, dxy, bxy);
-    const float vz = fmaf(kk.x, dz, bz);
-    const float2 txy = __fadd2_rn(vxy, magic2);
-    const float tz = __fadd_rn(vz, kMagic);
-    const float2 fxy = __fadd2_rn(txy, nmagic2);
-    const float fz = __fadd_rn(tz, -kMagic);
+    const float2 vxy = __ffma2_rn(kk, dxy, fr.bxy);
+    const float vz = fmaf(kk.x, dz, fr.bz);
+    const float2 txy = __fadd2_rn(vxy, fr.mxy);
+    const float tz = __fadd_rn(vz, fr.mz);
+    const float2 fxy = __ffma2_rn(fr.mxy, none2, txy);  // t - m, exact
+    const float fz = __fsub_rn(tz, fr.mz);
     const float2 hxy = __ffma2_rn(fxy, none2, vxy);
     const float hz = fmaf(fz, -1.0f, vz);
     uint32_t idx = __float_as_uint(txy.x) + __float_as_uint(txy.y) * sy + __float_as_uint(tz) * sz;
@@ -453,8 +482,7 @@ template <Accum ACC, int U>
 __device__ __forceinline__ void march_pairs(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
     const char* __restrict__ pairs = static_cast<const char*>(a.cells);
-    const float2 bxy = make_float2((float)r.base[0], (float)r.base[1]);
-    const float bz = (float)r.base[2];
+    const CellFrame fr = cell_frame(r);
     const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
     const float dz = (float)r.step[2];
     const uint32_t sy = a.csy, sz = a.csz, pmax = a.cmax;
@@ -466,13 +494,13 @@ __device__ __forceinline__ void march_pairs(const ProjectArgs& a, const Ray& r, 
         float part = 0.0f;
 #pragma unroll
         for (int j = 0; j < U; ++j) {
-            part += pair_sample(pairs, kk, bxy, bz, dxy, dz, sy, sz, pmax, pc);
+            part += pair_sample(pairs, kk, fr, dxy, dz, sy, sz, pmax, pc);
             kk = __fadd2_rn(kk, one2);
         }
         acc.add(part);
     }
     for (; k < r.n; ++k) {
-        acc.add(pair_sample(pairs, kk, bxy, bz, dxy, dz, sy, sz, pmax, pc));
+        acc.add(pair_sample(pairs, kk, fr, dxy, dz, sy, sz, pmax, pc));
         kk = __fadd2_rn(kk, one2);
     }
 }
