@@ -171,7 +171,7 @@ void CudaRayCasterProjector::setParameter(const QVariant& parameter)
     _settings.interpolate = map.value("Interpolate", true).toBool();
     _settings.device = map.value("Device", 0).toInt();
     _settings.interpolationMode = map.value("Interpolation mode", int(CTLCU_INTERP_SOFTWARE)).toInt();
-    _settings.accumulation = map.value("Accumulation", int(CTLCU_ACCUM_FP64)).toInt();
+    _settings.accumulation = map.value("Accumulation", int(CTLCU_ACCUM_KAHAN)).toInt();
     _settings.storage = map.value("Storage", int(CTLCU_F32)).toInt();
     _settings.kernel = map.value("Kernel", int(CTLCU_KERNEL_AUTO)).toInt();
 }

@@ -37,7 +37,7 @@ public:
         uint volumeUpSampling = 1;                  //!< 0: mean voxel, 1: as is, f: f^3 replication
         bool interpolate = true;                    //!< trilinear (true) or nearest voxel (false)
         int interpolationMode = CTLCU_INTERP_SOFTWARE; //!< software FP32 or hardware texture filter
-        int accumulation = CTLCU_ACCUM_FP64;        //!< FP64, Kahan FP32 or plain FP32
+        int accumulation = CTLCU_ACCUM_KAHAN;       //!< FP64, Kahan FP32 or plain FP32
         int storage = CTLCU_F32;                    //!< device storage of the volume (F32, BF16, F16)
         int kernel = CTLCU_KERNEL_AUTO;             //!< sample-loop variant
 

@@ -943,7 +943,7 @@ ctlcu_settings ctlcu_settings_default(void)
     s.volume_upsampling = 1;
     s.interpolate = 1;
     s.interp_mode = CTLCU_INTERP_SOFTWARE;
-    s.accum = CTLCU_ACCUM_FP64;
+    s.accum = CTLCU_ACCUM_KAHAN;
     s.kernel = CTLCU_KERNEL_AUTO;
     s.views_per_block = s.lanes_x = s.block_rays = s.unroll = 0;  // tuned or default launch shape
     return s;

@@ -84,7 +84,7 @@ class Settings:
     volume_upsampling: int = 1
     interpolate: bool = True
     interp_mode: int = L.INTERP_SOFTWARE
-    accum: int = L.ACCUM_FP64
+    accum: int = L.ACCUM_KAHAN
     storage: int = L.F32
     kernel: int = L.KERNEL_AUTO
     # launch shape (0 = autotuned for the volume and detector, else the default)
@@ -645,7 +645,7 @@ class CudaRayCasterProjector:
         s.interp_mode = L.INTERP_TEXTURE if m.get("Interpolation mode", "software") == "texture" \
             else L.INTERP_SOFTWARE
         s.accum = {"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[
-            m.get("Accumulation", "fp64")]
+            m.get("Accumulation", "kahan")]
         s.storage = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[m.get("Storage", "f32")]
 
     def to_variant(self) -> dict:

@@ -59,7 +59,7 @@ typedef enum {
 
 typedef enum {
     CTLCU_ACCUM_FP64 = 0,  /* double accumulator, as raycasterprojector_interp.cl:48,66 */
-    CTLCU_ACCUM_KAHAN = 1, /* float with compensated (Kahan) summation */
+    CTLCU_ACCUM_KAHAN = 1, /* float with compensated (Kahan) summation (default) */
     CTLCU_ACCUM_FP32 = 2   /* plain float */
 } ctlcu_accum;
 
@@ -91,9 +91,10 @@ typedef struct {
 
 /*
  * RayCasterProjector::Settings (raycasterprojector.h:27-37) plus the
- * B200 options.  ctlcu_settings_default() gives the reference defaults:
- * rays {1,1}, raySampling 0.3, volumeUpSampling 1, interpolate on,
- * software interpolation, FP64 accumulation, automatic kernel choice.
+ * B200 options.  ctlcu_settings_default() gives the reference defaults
+ * (rays {1,1}, raySampling 0.3, volumeUpSampling 1, interpolate on) and,
+ * for the B200 options, software interpolation, FP32 accumulation with
+ * Kahan compensation, automatic kernel choice and launch shape.
  */
 typedef struct {
     uint32_t rays_per_pixel[2]; /* sub-rays along channel (x) and row (y), 1..64 */

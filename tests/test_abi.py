@@ -79,7 +79,7 @@ def test_default_settings_are_the_reference_defaults():
     assert list(s.rays_per_pixel) == [1, 1]
     assert abs(s.ray_sampling - 0.3) < 1e-7
     assert s.volume_upsampling == 1 and s.interpolate == 1
-    assert s.interp_mode == L.INTERP_SOFTWARE and s.accum == L.ACCUM_FP64
+    assert s.interp_mode == L.INTERP_SOFTWARE and s.accum == L.ACCUM_KAHAN
     # launch shape left to the autotuner / defaults
     assert (s.views_per_block, s.lanes_x, s.block_rays, s.unroll) == (0, 0, 0, 0)
 
