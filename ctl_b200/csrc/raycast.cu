@@ -78,9 +78,11 @@ struct Accumulator<Accum::F32> {
     __device__ __forceinline__ double value() const { return static_cast<double>(s); }
 };
 
-// One ray ready for the sample loop.  The trilinear and texture loops run in
-// FP32 from the rounded base/step; the nearest-voxel loop keeps FP64, because a
-// position error there moves a sample into the neighbouring voxel.
+// One ray ready for the sample loop.  The cell, pair and trilinear loops run in
+// FP32 relative to the ray's integer origin (CellFrame); the texture loop runs
+// from the rounded absolute base, its 8-bit filter weights being far coarser;
+// the nearest-voxel loop keeps FP64, because a position error there moves a
+// sample into the neighbouring voxel.
 struct Ray {
     double base[3];  // coordinate of the first sample in the loop's index space
     double step[3];  // one step in voxel units
