@@ -430,6 +430,20 @@ def run_single_config(args, name):
     ms = V / best * 1e3
     extra = {"forms_views_per_s": results, "tuned": shapes, "samples_per_step": samples,
              "gsamples_per_s": samples / (ms / 1e3) / 1e9}
+    if name == "c3":
+        # compulsory HBM traffic of one step: the FP32 volume read once and the
+        # projections written once; beside it, the derived cell array (32 B per
+        # cell, (n + 3) cells per axis) read once in place of the volume
+        nz, ny, nx = (int(n) for n in job.volume.shape)
+        out_bytes = V * M * job.rows * job.channels * 4
+        vol_bytes = nx * ny * nz * 4
+        cell_bytes = 32 * (nx + 3) * (ny + 3) * (nz + 3)
+        t = ms / 1e3
+        extra["hbm_compulsory"] = {
+            "bytes_per_step": vol_bytes + out_bytes, "gb_s": (vol_bytes + out_bytes) / t / 1e9,
+            "frac_of_hbm": (vol_bytes + out_bytes) / t / 1e9 / hbm_peak(), "hbm_peak_gb_s": hbm_peak(),
+            "with_cell_array": {"bytes_per_step": cell_bytes + out_bytes, "gb_s": (cell_bytes + out_bytes) / t / 1e9,
+                                "frac_of_hbm": (cell_bytes + out_bytes) / t / 1e9 / hbm_peak()}}
     if name == "c1" and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
