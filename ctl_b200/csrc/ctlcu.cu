@@ -20,6 +20,7 @@
 #include <tuple>
 #include <unordered_map>
 #include <vector>
+#include <initializer_list>
 
 using namespace ctlcu;
 
@@ -96,14 +97,45 @@ int fail(ctlcu_ctx* ctx, int code, const char* fmt, ...)
         }                                                                                         \
     } while (0)
 
-bool is_device_ptr(const void* p)
+// Where `p` lives, seen from the current device (every entry point makes its
+// context's device current before it looks): host memory, device memory the
+// current device's kernels may dereference (its own, or managed), or device
+// memory of another GPU.
+enum class Mem { Host, Local, Foreign };
+
+Mem mem_kind(const void* p)
 {
     cudaPointerAttributes attr;
     if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return Mem::Host;
     }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    if (attr.type == cudaMemoryTypeManaged)
+        return Mem::Local;
+    if (attr.type != cudaMemoryTypeDevice)
+        return Mem::Host;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+        cudaGetLastError();
+        return Mem::Foreign;
+    }
+    return attr.device == cur ? Mem::Local : Mem::Foreign;
+}
+
+// Device memory of the current device (see mem_kind).  Memory of another GPU
+// is not: entry points refuse it first with check_local.
+bool is_device_ptr(const void* p) { return mem_kind(p) == Mem::Local; }
+
+// CTLCU_ERR_INVALID_ARGUMENT if any of the pointers is device memory of a GPU
+// other than the context's (current) one: its kernels would dereference it
+// without peer access.  Null pointers pass (the callers check them).
+int check_local(ctlcu_ctx* ctx, std::initializer_list<const void*> ptrs)
+{
+    for (const void* p : ptrs)
+        if (p && mem_kind(p) == Mem::Foreign)
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                        "a buffer is device memory of another GPU than the context's (cuda:%d)", ctx->device);
+    return CTLCU_OK;
 }
 
 size_t dtype_size(int dtype) { return dtype == CTLCU_F32 ? 4 : 2; }
@@ -739,7 +771,8 @@ int prepare_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n, con
             return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "request %u: unknown volume handle %llu", i,
                         (unsigned long long)q.volume);
         if (!q.pmats || !q.out || !is_device_ptr(q.pmats) || !is_device_ptr(q.out))
-            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "request %u: pmats/out must be device memory", i);
+            return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT,
+                        "request %u: pmats/out must be device memory of the context's GPU (cuda:%d)", i, ctx->device);
     }
     bp.persistent = s->interpolate && s->interp_mode == CTLCU_INTERP_SOFTWARE && s->volume_upsampling == 1 &&
                     s->kernel != CTLCU_KERNEL_GATHER;
@@ -836,6 +869,9 @@ std::mutex g_noalloc_mu;
 ViewGeom* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the context's device, which is current.
+// Looked up once per device and kept: it belongs to the device's primary
+// context, so it does not survive a cudaDeviceReset of that device (documented
+// at ctlcu_project_noalloc).
 int noalloc_scratch(ctlcu_ctx* ctx, ViewGeom** out)
 {
     if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
@@ -877,6 +913,8 @@ const char* missing_array(const VolumeEntry& v, const ctlcu_settings* s)
 template <typename Op>
 int on_device_data(ctlcu_ctx* ctx, float* data, size_t bytes, void* stream, const char* what, Op op)
 {
+    if (int r = check_local(ctx, { data }))
+        return r;
     const bool dev = is_device_ptr(data);
     cudaStream_t st = dev && stream ? (cudaStream_t)stream : ctx->stream;
     float* d = data;
@@ -1132,6 +1170,9 @@ int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* setting
     if (!v)
         return fail(ctx, CTLCU_ERR_INVALID_HANDLE, "unknown volume handle %llu", (unsigned long long)volume);
     cudaSetDevice(ctx->device);
+    r = check_local(ctx, { pmats, out });
+    if (r)
+        return r;
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     return project_any(ctx, *v, settings, pmats, n_views, n_modules, channels, rows, out, st, false);
 }
@@ -1156,6 +1197,9 @@ int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const fl
     if (r)
         return r;
     cudaSetDevice(ctx->device);
+    r = check_local(ctx, { volume, pmats, out });
+    if (r)
+        return r;
     VolumeEntry v;
     r = make_volume(ctx, desc, volume, is_device_ptr(volume), true, v);
     if (r == CTLCU_OK)
@@ -1361,6 +1405,8 @@ int ctlcu_count_samples(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* s
     const size_t pm_bytes = sizeof(double) * 12 * (size_t)n_views * n_modules;
     double* d_pm = nullptr;
     ViewGeom* geom = nullptr;
+    if (int rc = check_local(ctx, { pmats }))
+        return rc;
     const bool pm_dev = is_device_ptr(pmats);
     if (!pm_dev) {
         CU_TRY(ctx, cudaMallocAsync((void**)&d_pm, pm_bytes, st));
@@ -1416,6 +1462,8 @@ int ctlcu_autotune(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settin
     // job's regime rather than a part-empty grid; the job caps it.
     const size_t per_view = (size_t)n_modules * 12;
     std::vector<double> hp((size_t)n_views * per_view);
+    if (int rc = check_local(ctx, { pmats }))
+        return rc;
     if (is_device_ptr(pmats))
         CU_TRY(ctx, cudaMemcpy(hp.data(), pmats, hp.size() * sizeof(double), cudaMemcpyDeviceToHost));
     else
@@ -1801,7 +1849,7 @@ int ctlcu_den_write(ctlcu_ctx* ctx, const char* path, const void* data, uint32_t
     TraceRange trace_("ctlcu_den_write");
     if (!ctx) {
         // host data needs no context (nor a GPU)
-        if (!path || !data || is_device_ptr(data))
+        if (!path || !data || mem_kind(data) != Mem::Host)
             return CTLCU_ERR_INVALID_ARGUMENT;
         std::string msg;
         return den_write(path, data, elem_bytes, rows, cols, count, nullptr, nullptr, msg);
@@ -1822,7 +1870,7 @@ int ctlcu_nrrd_write_projections(ctlcu_ctx* ctx, const char* path, const float* 
     TraceRange trace_("ctlcu_nrrd_write_projections");
     std::string msg;
     if (!ctx) {
-        if (!path || !data || is_device_ptr(data))
+        if (!path || !data || mem_kind(data) != Mem::Host)
             return CTLCU_ERR_INVALID_ARGUMENT;
         return nrrd_write_projections(path, data, n_views, n_modules, rows, channels, nullptr, nullptr, msg);
     }
@@ -1859,7 +1907,7 @@ int ctlcu_nrrd_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capac
     TraceRange trace_("ctlcu_nrrd_read");
     std::string msg;
     if (!ctx) {
-        if (!path || !data || is_device_ptr(data))
+        if (!path || !data || mem_kind(data) != Mem::Host)
             return CTLCU_ERR_INVALID_ARGUMENT;
         return nrrd_read(path, data, capacity_bytes, nullptr, nullptr, msg);
     }
@@ -1884,7 +1932,7 @@ int ctlcu_den_read(ctlcu_ctx* ctx, const char* path, void* data, uint64_t capaci
 {
     TraceRange trace_("ctlcu_den_read");
     if (!ctx) {
-        if (!path || !data || is_device_ptr(data))
+        if (!path || !data || mem_kind(data) != Mem::Host)
             return CTLCU_ERR_INVALID_ARGUMENT;
         std::string msg;
         return den_read(path, data, capacity_bytes, first, n, nullptr, nullptr, msg);
@@ -2042,6 +2090,8 @@ int ctlcu_encode_geometry_shifted(ctlcu_ctx* ctx, const ctlcu_detector_desc* det
     if (n > 0x7fffffffull)
         return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "too many matrices");
     cudaSetDevice(ctx->device);
+    if (int rc = check_local(ctx, { pmats }))
+        return rc;
     const bool dev = is_device_ptr(pmats);
     cudaStream_t st = dev && stream ? (cudaStream_t)stream : ctx->stream;
     double* out = pmats;

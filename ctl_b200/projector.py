@@ -64,6 +64,36 @@ def _is_cuda(x) -> bool:
     return _is_torch(x) and x.is_cuda
 
 
+def _check_device_tensor(x, name: str, dtype: str, ndim: int, device: int) -> None:
+    """Raise ValueError unless x is a contiguous torch CUDA tensor of `dtype`
+    with `ndim` dimensions on CUDA device `device`: a buffer the kernels may
+    index by its shape alone."""
+    if not _is_cuda(x):
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if str(x.dtype) != f"torch.{dtype}":
+        raise ValueError(f"{name} must be {dtype}, got {x.dtype}")
+    if x.dim() != ndim:
+        raise ValueError(f"{name} must have {ndim} dimensions, got shape {tuple(x.shape)}")
+    if not x.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if x.device.index != device:
+        raise ValueError(f"{name} is on cuda:{x.device.index}, the context on cuda:{device}")
+
+
+def _check_out(out, V: int, M: int, rows: int, channels: int) -> None:
+    """A caller-supplied projection buffer must hold exactly [V][M][rows][channels]
+    float32 values in that order, or the kernel would write past it."""
+    shape = tuple(out.shape)
+    want = (V, M, rows, channels)
+    if shape != want:
+        raise ValueError(f"out must be shaped {want} (views, modules, rows, channels), got {shape}")
+    if _is_torch(out):
+        if str(out.dtype) != "torch.float32" or not out.is_contiguous():
+            raise ValueError("out must be a contiguous float32 tensor")
+    elif out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+        raise ValueError("out must be a C-contiguous float32 array")
+
+
 def torch_stream_handle(stream) -> int:
     """The C-ABI stream argument for a torch CUDA stream.  torch's default
     stream has the handle 0, which the C ABI reads as the context's own
@@ -348,6 +378,8 @@ class Context:
         V, M = int(P.shape[0]), int(P.shape[1])
         if out is None:
             out = self._out_like(P, V, M, rows, channels)
+        else:
+            _check_out(out, V, M, int(rows), int(channels))
         st = settings.to_c()
         stream = self._stream_for(stream, P, out)
         self._check(self.lib.ctlcu_project(self.h, volume.handle, C.byref(st), C.c_void_p(_ptr(P)), V, M,
@@ -360,8 +392,17 @@ class Context:
         """ctlcu_project_noalloc, for callers that cannot allocate device memory
         during the call: device pmats (V,M,3,4) f64 and out (V,M,R,C) f32; the
         ray geometry goes into the library's static scratch array (at most
-        NOALLOC_MAX_VIEW_MODULES view-modules per call)."""
+        NOALLOC_MAX_VIEW_MODULES view-modules per call).  Nothing is converted
+        or copied here (that would allocate), so tensors of the wrong type,
+        layout, shape or device raise ValueError instead of reaching the kernel."""
         settings = settings or Settings()
+        _check_device_tensor(pmats, "pmats", "float64", 4, self.device)
+        _check_device_tensor(out, "out", "float32", 4, self.device)
+        if tuple(pmats.shape[2:]) != (3, 4):
+            raise ValueError(f"pmats must be shaped (views, modules, 3, 4), got {tuple(pmats.shape)}")
+        if tuple(out.shape[:2]) != tuple(pmats.shape[:2]):
+            raise ValueError(f"out must be shaped (views, modules, rows, channels) with the views and modules "
+                             f"of pmats {tuple(pmats.shape[:2])}, got {tuple(out.shape)}")
         V, M = int(pmats.shape[0]), int(pmats.shape[1])
         R, Ch = int(out.shape[2]), int(out.shape[3])
         st = settings.to_c()
@@ -464,6 +505,8 @@ class Context:
         V, M = int(P.shape[0]), int(P.shape[1])
         if out is None:
             out = self._out_like(P, V, M, rows, channels)
+        else:
+            _check_out(out, V, M, int(rows), int(channels))
         desc = vol.desc(settings.storage)
         st = settings.to_c()
         self._check(self.lib.ctlcu_project_volume(self.h, C.byref(desc), C.c_void_p(_ptr(data)), C.byref(st),

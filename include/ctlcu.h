@@ -46,7 +46,7 @@ typedef enum {
     CTLCU_ERR_CUDA = 4,             /* a CUDA runtime call failed */
     CTLCU_ERR_NO_DEVICE = 5,        /* device index out of range / no CUDA device */
     CTLCU_ERR_SINGULAR_GEOMETRY = 6,/* a projection matrix had a singular M; its pixels are 0 */
-    CTLCU_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+    CTLCU_ERR_TIMEOUT = 7,          /* reserved: no call returns it (no kernel here waits on a device-side flag) */
     CTLCU_ERR_BUSY = 8              /* admission refused (queue full) */
 } ctlcu_status;
 
@@ -495,6 +495,9 @@ CTLCU_API int ctlcu_spectral_combine_noisy(ctlcu_ctx* ctx, const float* material
  *    otherwise CTLCU_ERR_INVALID_ARGUMENT names the missing one.
  *  - The first call on a device looks up the scratch array's address there
  *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    The address is kept for the life of the process: after cudaDeviceReset
+ *    (or any teardown of the device's primary context) this call must not be
+ *    used on that device again.
  *  - Every call on a device shares the one scratch array: calls whose work
  *    overlaps on the GPU (on different streams or contexts) race on it, so
  *    serialise them (one stream, or events between them).

@@ -14,7 +14,6 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_REF_DIR = "/root/reference"
 
 
 class _Volume(C.Structure):
@@ -26,13 +25,12 @@ class _Settings(C.Structure):
                 ("volume_upsampling", C.c_uint), ("interpolate", C.c_int)]
 
 
-def build(with_ref: bool | None = None) -> None:
-    """Compile liboracle.so, and _ref/libctlref.so when the reference is present."""
+def build(with_ref: bool = True) -> None:
+    """Compile liboracle.so, and _ref/libctlref.so where the reference sources
+    are present (the Makefile's REF, overridable by CTL_REFERENCE_DIR)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if with_ref is None:
-        with_ref = os.path.isdir(_REF_DIR)
     if with_ref:
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={_REF_DIR}"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref-if-present"], check=True)
 
 
 _libs: dict = {}

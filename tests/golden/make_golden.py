@@ -1,11 +1,12 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
+    export CTL_REFERENCE_DIR=/root/reference   # the reference's source tree
     make -C oracle all ref          # builds oracle/_ref/libctlref.so from the reference sources
     python tests/golden/make_golden.py          # everything
     python tests/golden/make_golden.py den      # den_files.json only
 
-Needs the reference sources at /root/reference (only where this script runs;
-the tests read the .npz files it writes, never the reference).
+Needs the reference sources, located by CTL_REFERENCE_DIR (only where this
+script runs; the tests read the fixtures it writes, never the reference).
 
 Writes
   geometry.npz     CTL's golden FullGeometry test data (testing/testData/tubeGeo.den,
@@ -40,7 +41,10 @@ from ctl_b200 import geometry as G  # noqa: E402
 from ctl_b200 import phantom as Ph  # noqa: E402
 from ctl_b200.den import read_full_geometry  # noqa: E402
 
-TESTDATA = "/root/reference/testing/testData"
+REF = os.environ.get("CTL_REFERENCE_DIR")
+if not REF:
+    sys.exit("make_golden.py: set CTL_REFERENCE_DIR to the reference's source tree")
+TESTDATA = os.path.join(REF, "testing", "testData")
 
 
 def cases():
