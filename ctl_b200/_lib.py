@@ -100,6 +100,9 @@ SIGNATURES = [
                                       C.POINTER(C.c_uint64)]),
     ("ctlcu_volume_release", C.c_int, [C.c_void_p, C.c_uint64]),
     ("ctlcu_volume_bytes", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ctlcu_set_volume_cache", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("ctlcu_volume_cache_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_uint32)]),
     ("ctlcu_project", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                 C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("ctlcu_project_noalloc", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
@@ -155,6 +158,16 @@ SIGNATURES = [
     ("ctlcu_nrrd_read", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("ctlcu_den_read", C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32,
                                  C.c_void_p]),
+    ("ctlcu_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("ctlcu_group_create", C.c_int, [C.POINTER(C.c_int), C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("ctlcu_group_destroy", C.c_int, [C.c_void_p]),
+    ("ctlcu_group_last_error", C.c_char_p, [C.c_void_p]),
+    ("ctlcu_group_size", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    ("ctlcu_group_context", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("ctlcu_group_project_volume", C.c_int, [C.c_void_p, C.POINTER(VolumeDesc), C.c_void_p, C.POINTER(Settings),
+                                             C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                             C.c_void_p]),
+    ("ctlcu_split_views", C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
 ]
 
 _lib = None
@@ -188,3 +201,23 @@ def check(status: int, ctx=None) -> None:
     if status != OK:
         msg = load().ctlcu_last_error(ctx).decode() if ctx else ""
         raise CtlcuError(status, msg)
+
+
+def check_group(status: int, group) -> None:
+    if status != OK:
+        raise CtlcuError(status, load().ctlcu_group_last_error(group).decode())
+
+
+def device_count() -> int:
+    """ctlcu_device_count: CUDA devices this process sees."""
+    n = C.c_int(0)
+    check(load().ctlcu_device_count(C.byref(n)))
+    return int(n.value)
+
+
+def split_views(n_views: int, n_parts: int) -> list:
+    """ctlcu_split_views: the first view of each of n_parts contiguous blocks,
+    plus n_views at the end (n_parts + 1 entries)."""
+    first = (C.c_uint32 * (n_parts + 1))()
+    check(load().ctlcu_split_views(int(n_views), int(n_parts), first))
+    return list(first)

@@ -14,20 +14,33 @@ DECLARE_SERIALIZABLE_TYPE(CudaRayCasterProjector)
 
 // The reference constructor throws std::runtime_error when OpenCL or its
 // kernels are missing (raycasterprojector.cpp:388-422); this one throws when
-// no CUDA device can be bound.
-CudaRayCasterProjector::CudaRayCasterProjector()
-{
-    const int rc = ctlcu_create(_settings.device, &_ctx);
-    if(rc != CTLCU_OK)
-        throw std::runtime_error("CudaRayCasterProjector: no usable CUDA device (ctlcu status " +
-                                 std::to_string(rc) + ")");
-    _ctxDevice = _settings.device;
-}
+// no CUDA device can be bound.  Like OpenCLConfig, it binds every device of
+// the (default, empty = all) device list up front.
+CudaRayCasterProjector::CudaRayCasterProjector() { ensureGroup(); }
 
 CudaRayCasterProjector::~CudaRayCasterProjector()
 {
-    if(_ctx)
-        ctlcu_destroy(_ctx);
+    if(_group)
+        ctlcu_group_destroy(_group);
+}
+
+// One context per listed device, rebuilt when deviceIDs changes; an ordinal
+// that does not exist throws, as prepareOpenCLDeviceList does
+// (raycasterprojector.cpp:434-461).
+void CudaRayCasterProjector::ensureGroup()
+{
+    if(_group && _groupIDs == _settings.deviceIDs)
+        return;
+    std::vector<int> ids(_settings.deviceIDs.begin(), _settings.deviceIDs.end());
+    ctlcu_group* group = nullptr;
+    const int rc = ctlcu_group_create(ids.data(), uint32_t(ids.size()), &group);
+    if(rc != CTLCU_OK)
+        throw std::runtime_error("CudaRayCasterProjector: device ID is not available or no usable CUDA "
+                                 "device (ctlcu status " + std::to_string(rc) + ")");
+    if(_group)
+        ctlcu_group_destroy(_group);
+    _group = group;
+    _groupIDs = _settings.deviceIDs;
 }
 
 // raycasterprojector.cpp:97-107
@@ -90,14 +103,17 @@ ProjectionData CudaRayCasterProjector::project(const VolumeData& volume)
         qCritical() << "CudaRayCasterProjector::project: no views configured";
         return ret;
     }
-    if(_ctxDevice != _settings.device)
+    ensureGroup();
+    // repeated projections of one volume (extensions re-projecting it per
+    // focal-spot sample or energy bin, a registration loop per pose) reuse the
+    // device copy instead of uploading it again; results are the same
+    uint32_t nbDevices = 0;
+    ctlcu_group_size(_group, &nbDevices);
+    for(uint32_t i = 0; i < nbDevices; ++i)
     {
         ctlcu_ctx* ctx = nullptr;
-        if(ctlcu_create(_settings.device, &ctx) != CTLCU_OK)
-            throw std::runtime_error("CudaRayCasterProjector: device ID is not available.");
-        ctlcu_destroy(_ctx);
-        _ctx = ctx;
-        _ctxDevice = _settings.device;
+        if(ctlcu_group_context(_group, i, &ctx) == CTLCU_OK)
+            ctlcu_set_volume_cache(ctx, _settings.volumeCacheSize);
     }
 
     ctlcu_volume_desc desc;
@@ -115,13 +131,15 @@ ProjectionData CudaRayCasterProjector::project(const VolumeData& volume)
     const size_t pixelsPerModule = size_t(_viewDim.nbRows) * _viewDim.nbChannels;
     std::vector<float> out(size_t(nbViews) * _viewDim.nbModules * pixelsPerModule, 0.0f);
     const ctlcu_settings s = cSettings();
-    const int rc = ctlcu_project_volume(_ctx, &desc, volume.rawData(), &s, _pmatBuffer.data(), nbViews,
-                                        _viewDim.nbModules, _viewDim.nbChannels, _viewDim.nbRows,
-                                        out.data());
+    // views in contiguous blocks over the listed devices (raycasterprojector.cpp:321-357
+    // deals them out round-robin); one device runs the call on the caller's thread
+    const int rc = ctlcu_group_project_volume(_group, &desc, volume.rawData(), &s, _pmatBuffer.data(), nbViews,
+                                              _viewDim.nbModules, _viewDim.nbChannels, _viewDim.nbRows,
+                                              out.data());
     if(rc != CTLCU_OK && rc != CTLCU_ERR_SINGULAR_GEOMETRY)
-        qCritical() << "ctlcu error" << rc << ":" << ctlcu_last_error(_ctx);
+        qCritical() << "ctlcu error" << rc << ":" << ctlcu_group_last_error(_group);
     else if(rc == CTLCU_ERR_SINGULAR_GEOMETRY)
-        qWarning() << "QR decomposition: matrix is close to singular;" << ctlcu_last_error(_ctx);
+        qWarning() << "QR decomposition: matrix is close to singular;" << ctlcu_group_last_error(_group);
 
     ret.allocateMemory(nbViews);
     const float* src = out.data();
@@ -153,7 +171,6 @@ QVariant CudaRayCasterProjector::parameter() const
     ret.insert("Ray sampling step length", _settings.raySampling);
     ret.insert("Volume upsampling factor", _settings.volumeUpSampling);
     ret.insert("Interpolate", _settings.interpolate);
-    ret.insert("Device", _settings.device);
     ret.insert("Interpolation mode", _settings.interpolationMode);
     ret.insert("Accumulation", _settings.accumulation);
     ret.insert("Storage", _settings.storage);
@@ -169,7 +186,6 @@ void CudaRayCasterProjector::setParameter(const QVariant& parameter)
     _settings.raySampling = map.value("Ray sampling step length", 0.3f).toFloat();
     _settings.volumeUpSampling = map.value("Volume upsampling factor", 1u).toUInt();
     _settings.interpolate = map.value("Interpolate", true).toBool();
-    _settings.device = map.value("Device", 0).toInt();
     _settings.interpolationMode = map.value("Interpolation mode", int(CTLCU_INTERP_SOFTWARE)).toInt();
     _settings.accumulation = map.value("Accumulation", int(CTLCU_ACCUM_KAHAN)).toInt();
     _settings.storage = map.value("Storage", int(CTLCU_F32)).toInt();

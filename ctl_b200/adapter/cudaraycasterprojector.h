@@ -31,7 +31,8 @@ public:
     class Settings
     {
     public:
-        int device = 0;                             //!< CUDA device index
+        std::vector<uint> deviceIDs;                //!< CUDA device ordinals (if empty: use all), as
+                                                    //!< RayCasterProjector::Settings::deviceIDs
         uint raysPerPixel[2] = { 1, 1 };            //!< sub-rays per pixel along channels (x) and rows (y)
         float raySampling = 0.3f;                   //!< step as a fraction of the smallest voxel size
         uint volumeUpSampling = 1;                  //!< 0: mean voxel, 1: as is, f: f^3 replication
@@ -40,6 +41,8 @@ public:
         int accumulation = CTLCU_ACCUM_KAHAN;       //!< FP64, Kahan FP32 or plain FP32
         int storage = CTLCU_F32;                    //!< device storage of the volume (F32, BF16, F16)
         int kernel = CTLCU_KERNEL_AUTO;             //!< sample-loop variant
+        uint volumeCacheSize = 4;                   //!< resident copies of recently projected volumes kept
+                                                    //!< per device (0: upload every call, as the reference)
 
         static Settings optimizedFor(const VolumeData& volume, const AbstractDetector& detector);
     };
@@ -63,8 +66,10 @@ private:
     SingleViewData::Dimensions _viewDim;
     FullGeometry _pMats;
     std::vector<double> _pmatBuffer;  //!< [view][module] row-major 3x4 matrices
-    ctlcu_ctx* _ctx = nullptr;
-    int _ctxDevice = -1;
+    void ensureGroup();
+
+    ctlcu_group* _group = nullptr;    //!< one context per device of _groupIDs
+    std::vector<uint> _groupIDs;      //!< deviceIDs the group was made for
 };
 
 } // namespace CUDA

@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -71,6 +72,17 @@ struct ctlcu_ctx {
     std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, Tuned> tuned;
     DenStaging den;  // pinned buffers for DEN file streaming, allocated on first use
     cudaStream_t copy_stream = nullptr;  // device-to-host copies that overlap projection
+    // ctlcu_project_volume's resident copies of host volumes (ctlcu_set_volume_cache):
+    // the volume's description and a hash of its whole content identify it
+    struct Cached {
+        ctlcu_volume_desc desc;
+        uint64_t hash;
+        uint64_t handle;  // in `vols`, never handed to the caller
+        uint64_t last;    // use clock, for least-recently-used eviction
+    };
+    std::vector<Cached> cache;
+    uint32_t cache_max = 0;  // 0: every call uploads its volume (the reference's behaviour)
+    uint64_t cache_clock = 0, cache_hits = 0, cache_misses = 0;
 };
 
 namespace {
@@ -737,6 +749,138 @@ int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const d
     return CTLCU_OK;
 }
 
+// ---- the volume cache of ctlcu_project_volume ---------------------------------------------------
+
+// 64-bit hash of n floats: four interleaved multiply-rotate accumulators over
+// 8-byte words (the round of the published XXH64 algorithm), merged with a
+// final avalanche.  Large volumes are hashed by several host threads in
+// fixed-size chunks, whose hashes are then hashed in order, so the result
+// does not depend on the thread count.
+uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+
+constexpr uint64_t kP1 = 11400714785074694791ull, kP2 = 14029467366897019727ull, kP3 = 1609587929392839161ull;
+
+uint64_t mix64(uint64_t h)
+{
+    h ^= h >> 33;
+    h *= kP2;
+    h ^= h >> 29;
+    h *= kP3;
+    h ^= h >> 32;
+    return h;
+}
+
+// n 8-byte words at p (any alignment: each word is read with memcpy, one
+// unaligned load on the host CPU).
+uint64_t hash_words(const unsigned char* p, size_t n, uint64_t seed)
+{
+    auto word = [p](size_t i) {
+        uint64_t x;
+        std::memcpy(&x, p + 8 * i, 8);
+        return x;
+    };
+    uint64_t a[4] = { seed + kP1 + kP2, seed + kP2, seed, seed - kP1 };
+    size_t i = 0;
+    for (; i + 4 <= n; i += 4)
+        for (int k = 0; k < 4; ++k)
+            a[k] = rotl64(a[k] + word(i + k) * kP2, 31) * kP1;
+    uint64_t h = rotl64(a[0], 1) + rotl64(a[1], 7) + rotl64(a[2], 12) + rotl64(a[3], 18);
+    for (; i < n; ++i)
+        h = rotl64(h ^ (rotl64(word(i) * kP2, 31) * kP1), 27) * kP1 + kP3;
+    return mix64(h ^ (uint64_t)n);
+}
+
+uint64_t volume_hash(const ctlcu_volume_desc* d, const float* data)
+{
+    const size_t n = (size_t)d->n[0] * d->n[1] * d->n[2];
+    const size_t words = n / 2;
+    const unsigned char* bytes = reinterpret_cast<const unsigned char*>(data);
+    constexpr size_t kChunk = size_t(1) << 21;  // words per chunk (16 MiB)
+    const size_t chunks = (words + kChunk - 1) / kChunk;
+    std::vector<uint64_t> part(chunks + 2, 0);
+    auto run = [&](size_t c0, size_t c1) {
+        for (size_t c = c0; c < c1; ++c) {
+            const size_t w0 = c * kChunk, nw = std::min(kChunk, words - w0);
+            part[c] = hash_words(bytes + 8 * w0, nw, c);
+        }
+    };
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min<size_t>(hw, chunks);
+    if (nt <= 1) {
+        run(0, chunks);
+    } else {
+        std::vector<std::thread> ts;
+        for (size_t t = 0; t < nt; ++t)
+            ts.emplace_back(run, chunks * t / nt, chunks * (t + 1) / nt);
+        for (auto& t : ts)
+            t.join();
+    }
+    uint32_t tail = 0;
+    if (n & 1)
+        std::memcpy(&tail, data + n - 1, 4);
+    part[chunks] = tail;
+    unsigned char desc_bytes[48];
+    std::memset(desc_bytes, 0, sizeof desc_bytes);
+    std::memcpy(desc_bytes, d, std::min(sizeof desc_bytes, sizeof *d));
+    part[chunks + 1] = hash_words(desc_bytes, 6, 0x9e3779b97f4a7c15ull);
+    return hash_words(reinterpret_cast<const unsigned char*>(part.data()), part.size(), 0);
+}
+
+bool same_desc(const ctlcu_volume_desc& a, const ctlcu_volume_desc& b)
+{
+    for (int k = 0; k < 3; ++k)
+        if (a.n[k] != b.n[k] || a.voxel_mm[k] != b.voxel_mm[k] || a.offset_mm[k] != b.offset_mm[k])
+            return false;
+    return a.dtype == b.dtype;
+}
+
+void evict_cached(ctlcu_ctx* ctx, size_t i)
+{
+    const uint64_t h = ctx->cache[i].handle;
+    if (VolumeEntry* v = find_volume(ctx, h)) {
+        cudaStreamSynchronize(ctx->stream);
+        free_volume(ctx, *v);
+        ctx->vols.erase(h);
+    }
+    ctx->cache.erase(ctx->cache.begin() + (ptrdiff_t)i);
+}
+
+// The resident copy of host volume `data` in the cache, uploaded (and the least
+// recently used entry evicted) on a miss.
+int cached_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* d, const float* data, VolumeEntry** out)
+{
+    const uint64_t h = volume_hash(d, data);
+    for (auto& c : ctx->cache)
+        if (c.hash == h && same_desc(c.desc, *d)) {
+            if (VolumeEntry* v = find_volume(ctx, c.handle)) {
+                c.last = ++ctx->cache_clock;
+                ++ctx->cache_hits;
+                *out = v;
+                return CTLCU_OK;
+            }
+        }
+    ++ctx->cache_misses;
+    while (!ctx->cache.empty() && ctx->cache.size() >= ctx->cache_max) {
+        size_t lru = 0;
+        for (size_t i = 1; i < ctx->cache.size(); ++i)
+            if (ctx->cache[i].last < ctx->cache[lru].last)
+                lru = i;
+        evict_cached(ctx, lru);
+    }
+    VolumeEntry v;
+    int r = make_volume(ctx, d, data, false, false, v);
+    if (r) {
+        free_volume(ctx, v);
+        return r;
+    }
+    const uint64_t handle = ctx->next_handle++;
+    v.handle = handle;
+    ctx->vols.emplace(handle, v);
+    ctx->cache.push_back({ *d, h, handle, ++ctx->cache_clock });
+    *out = find_volume(ctx, handle);
+    return CTLCU_OK;
+}
+
 // ---- batches --------------------------------------------------------------------------------
 
 struct BatchPrep {
@@ -1150,6 +1294,37 @@ int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes)
     return CTLCU_OK;
 }
 
+int ctlcu_set_volume_cache(ctlcu_ctx* ctx, uint32_t max_volumes)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ctx->cache_max = max_volumes;
+    while (ctx->cache.size() > max_volumes) {
+        size_t lru = 0;
+        for (size_t i = 1; i < ctx->cache.size(); ++i)
+            if (ctx->cache[i].last < ctx->cache[lru].last)
+                lru = i;
+        evict_cached(ctx, lru);
+    }
+    return CTLCU_OK;
+}
+
+int ctlcu_volume_cache_stats(ctlcu_ctx* ctx, uint64_t* hits, uint64_t* misses, uint32_t* resident)
+{
+    if (!ctx)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (hits)
+        *hits = ctx->cache_hits;
+    if (misses)
+        *misses = ctx->cache_misses;
+    if (resident)
+        *resident = (uint32_t)ctx->cache.size();
+    return CTLCU_OK;
+}
+
 int ctlcu_project(ctlcu_ctx* ctx, uint64_t volume, const ctlcu_settings* settings, const double* pmats,
                   uint32_t n_views, uint32_t n_modules, uint32_t channels, uint32_t rows, float* out,
                   void* stream)
@@ -1200,6 +1375,15 @@ int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc, const fl
     r = check_local(ctx, { volume, pmats, out });
     if (r)
         return r;
+    if (ctx->cache_max && !is_device_ptr(volume)) {
+        // a host volume seen before (same description and content) is projected
+        // from its resident copy: no upload, no cell build
+        VolumeEntry* cv = nullptr;
+        r = cached_volume(ctx, desc, volume, &cv);
+        if (r == CTLCU_OK)
+            r = project_any(ctx, *cv, settings, pmats, n_views, n_modules, channels, rows, out, ctx->stream, true);
+        return r;
+    }
     VolumeEntry v;
     r = make_volume(ctx, desc, volume, is_device_ptr(volume), true, v);
     if (r == CTLCU_OK)

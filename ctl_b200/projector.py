@@ -117,6 +117,9 @@ class Settings:
     accum: int = L.ACCUM_KAHAN
     storage: int = L.F32
     kernel: int = L.KERNEL_AUTO
+    # resident copies of recently projected host volumes kept per device by the
+    # projector (0: upload every call, as the reference does)
+    volume_cache: int = 4
     # launch shape (0 = autotuned for the volume and detector, else the default)
     views_per_block: int = 0
     lanes_x: int = 0
@@ -342,6 +345,16 @@ class Context:
         return int(n.value)
 
     # ---- volumes --------------------------------------------------------------------------
+    def set_volume_cache(self, max_volumes: int) -> None:
+        """ctlcu_set_volume_cache: keep resident copies of the last max_volumes
+        distinct host volumes project_volume saw (0 = upload every call)."""
+        self._check(self.lib.ctlcu_set_volume_cache(self.h, int(max_volumes)))
+
+    def volume_cache_stats(self) -> dict:
+        hits, misses, resident = C.c_uint64(0), C.c_uint64(0), C.c_uint32(0)
+        self._check(self.lib.ctlcu_volume_cache_stats(self.h, C.byref(hits), C.byref(misses), C.byref(resident)))
+        return {"hits": int(hits.value), "misses": int(misses.value), "resident": int(resident.value)}
+
     def volume(self, vol: VoxelVolume, dtype: int = L.F32) -> Volume:
         data = _contig_f32(vol.data)
         desc = vol.desc(dtype)
@@ -597,12 +610,83 @@ class Context:
         return qr, src
 
 
+class Group:
+    """Several devices behind one projection (ctlcu_group): the B200 form of
+    RayCasterProjector::Settings::deviceIDs (raycasterprojector.h:30).  One
+    context per listed device ordinal (an empty list: every device, as in the
+    reference); project_volume gives each device a contiguous block of views
+    (ctlcu_split_views) with its own upload of the volume, and its result
+    equals a one-device call bit for bit."""
+
+    def __init__(self, devices: Sequence[int] = ()):
+        self.lib = L.load()
+        ids = [int(d) for d in devices]
+        arr = (C.c_int * max(1, len(ids)))(*ids)
+        h = C.c_void_p()
+        L.check(self.lib.ctlcu_group_create(arr, len(ids), C.byref(h)))
+        self.h = h
+        self.devices = tuple(ids)
+
+    def size(self) -> int:
+        n = C.c_uint32(0)
+        L.check_group(self.lib.ctlcu_group_size(self.h, C.byref(n)), self.h)
+        return int(n.value)
+
+    def set_volume_cache(self, max_volumes: int) -> None:
+        """ctlcu_set_volume_cache on every device's context of the group."""
+        for i in range(self.size()):
+            ctx = C.c_void_p()
+            L.check_group(self.lib.ctlcu_group_context(self.h, i, C.byref(ctx)), self.h)
+            L.check(self.lib.ctlcu_set_volume_cache(ctx, int(max_volumes)), ctx)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.ctlcu_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def project_volume(self, vol: VoxelVolume, pmats, channels: int, rows: int,
+                       settings: Optional[Settings] = None, out=None) -> np.ndarray:
+        """ctlcu_group_project_volume: host volume, pmats and output."""
+        settings = settings or Settings()
+        data = np.ascontiguousarray(vol.data, dtype=np.float32)
+        P = np.ascontiguousarray(pmats, dtype=np.float64)
+        V, M = int(P.shape[0]), int(P.shape[1])
+        if out is None:
+            out = np.empty((V, M, int(rows), int(channels)), np.float32)
+        else:
+            _check_out(out, V, M, int(rows), int(channels))
+        desc = vol.desc(settings.storage)
+        st = settings.to_c()
+        L.check_group(self.lib.ctlcu_group_project_volume(
+            self.h, C.byref(desc), C.c_void_p(data.ctypes.data), C.byref(st), C.c_void_p(P.ctypes.data), V, M,
+            int(channels), int(rows), C.c_void_p(out.ctypes.data)), self.h)
+        return out
+
+
 # ---------------------------------------------------------------------------------------------
 # the AbstractProjector mirror
 # ---------------------------------------------------------------------------------------------
 
 class CudaRayCasterProjector:
-    """Drop-in for CTL::OCL::RayCasterProjector on one B200."""
+    """Drop-in for CTL::OCL::RayCasterProjector on B200s.
+
+    ``settings().device_ids`` lists the devices a projection is spread over,
+    as the reference's deviceIDs (raycasterprojector.h:30; empty: every
+    device, raycasterprojector.cpp:449-454).  A list of just the context's
+    device (``device``, where the extensions keep their resident volumes)
+    projects on that context; any other list goes through a ``Group``."""
 
     TYPE_ID = 1  # CTL_TYPE_ID(1) of RayCasterProjector (raycasterprojector.h:22)
 
@@ -612,8 +696,19 @@ class CudaRayCasterProjector:
         # or binding the device raises
         self._settings = Settings()
         self._ctx = Context(device)
+        self._group: Optional[Group] = None
         self._geometry: Optional[AcquisitionGeometry] = None
         self.notifier: List[Callable[[int], None]] = []
+
+    def _group_for(self, ids) -> Group:
+        """The device group of this id list, rebuilt when the list changes; an
+        ordinal that does not exist raises (raycasterprojector.cpp:442-447)."""
+        if self._group is None or self._group.devices != tuple(ids):
+            if self._group is not None:
+                self._group.close()
+                self._group = None
+            self._group = Group(ids)
+        return self._group
 
     # ---- AbstractProjector ----------------------------------------------------------------
     def configure(self, setup: AcquisitionGeometry) -> None:
@@ -639,8 +734,17 @@ class CudaRayCasterProjector:
         if volume.smallest_voxel_size() <= 0.0:
             log.warning("voxel size is zero or negative")
         P = self._geometry.pmats
+        # the device list is checked before the projection, outside its error
+        # handling: a bad ordinal raises (raycasterprojector.cpp:142, :442-447)
+        ids = [int(d) for d in self._settings.device_ids] or list(range(L.device_count()))
+        group = self._group_for(ids) if ids != [self._ctx.device] else None
         try:
-            out = self._ctx.project_volume(volume, P, vd.nb_channels, vd.nb_rows, self._settings)
+            if group is not None:
+                group.set_volume_cache(self._settings.volume_cache)
+                out = group.project_volume(volume, P, vd.nb_channels, vd.nb_rows, self._settings)
+            else:
+                self._ctx.set_volume_cache(self._settings.volume_cache)
+                out = self._ctx.project_volume(volume, P, vd.nb_channels, vd.nb_rows, self._settings)
             ret.data = out
         except L.CtlcuError as e:
             log.critical("ctlcu error: %s", e)

@@ -155,6 +155,26 @@ CTLCU_API int ctlcu_volume_create(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc,
 CTLCU_API int ctlcu_volume_release(ctlcu_ctx* ctx, uint64_t handle);
 CTLCU_API int ctlcu_volume_bytes(ctlcu_ctx* ctx, uint64_t handle, uint64_t* bytes);
 
+/*
+ * Volume cache of ctlcu_project_volume (default 0 = off: every call uploads its
+ * volume and frees it, as RayCasterProjector::project does,
+ * raycasterprojector.cpp:239-269).  With max_volumes > 0 the context keeps
+ * resident copies (with their derived cell arrays) of the last max_volumes
+ * distinct host volumes it projected; a later call whose volume has the same
+ * description and the same content (a 64-bit hash of every voxel, computed on
+ * the host) projects from the resident copy, without upload or cell build.
+ * CTL's extensions re-project one volume many times (ArealFocalSpotExtension
+ * per focal-spot sample, SpectralEffectsExtension per energy bin,
+ * arealfocalspotextension.cpp:133-150, spectraleffectsextension.cpp:385-391),
+ * and registration loops project one volume per pose.  Results are the same
+ * with and without the cache.  The least recently used copy is evicted first;
+ * setting a smaller size evicts at once.  Cached copies count against the
+ * memory budget.  Device-memory volumes are never cached.
+ */
+CTLCU_API int ctlcu_set_volume_cache(ctlcu_ctx* ctx, uint32_t max_volumes);
+/* Calls served from the cache, calls that uploaded, and copies now resident (each may be NULL). */
+CTLCU_API int ctlcu_volume_cache_stats(ctlcu_ctx* ctx, uint64_t* hits, uint64_t* misses, uint32_t* resident);
+
 /* ---- projection -------------------------------------------------------------------------- */
 
 /*
@@ -199,6 +219,48 @@ CTLCU_API int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, u
                                 const ctlcu_settings* settings, ctlcu_plan** plan);
 CTLCU_API int ctlcu_plan_launch(ctlcu_plan* plan, void* stream);
 CTLCU_API int ctlcu_plan_destroy(ctlcu_plan* plan);
+
+/* ---- several devices ---------------------------------------------------------------------- */
+
+/*
+ * RayCasterProjector::Settings::deviceIDs (raycasterprojector.h:30): one
+ * projection spread over several devices.  A group holds one context per
+ * listed device ordinal (n_devices = 0: every device, as an empty deviceIDs
+ * list means in the reference, raycasterprojector.cpp:449-454; an ordinal may
+ * be listed more than once).  An unavailable ordinal fails with
+ * CTLCU_ERR_NO_DEVICE, like prepareOpenCLDeviceList (:434-461).
+ */
+typedef struct ctlcu_group ctlcu_group;
+/* Number of CUDA devices this process sees (0 when there is none). */
+CTLCU_API int ctlcu_device_count(int* n);
+CTLCU_API int ctlcu_group_create(const int* devices, uint32_t n_devices, ctlcu_group** out);
+CTLCU_API int ctlcu_group_destroy(ctlcu_group* group);
+CTLCU_API const char* ctlcu_group_last_error(const ctlcu_group* group);
+CTLCU_API int ctlcu_group_size(const ctlcu_group* group, uint32_t* n_devices);
+/* The context of the group's index-th device (owned by the group), for
+ * per-device settings such as a memory budget. */
+CTLCU_API int ctlcu_group_context(ctlcu_group* group, uint32_t index, ctlcu_ctx** ctx);
+
+/*
+ * The reference's multi-device RayCasterProjector::project
+ * (raycasterprojector.cpp:187-208, :239-251, :321-357) with the argument
+ * meaning of ctlcu_project_volume; volume, pmats and out are host memory.
+ * min(#devices, n_views) devices take part; device i projects the contiguous
+ * block of views [first[i], first[i+1]) of ctlcu_split_views with its own
+ * upload of the volume, in its own host thread, into its own slice of `out`.
+ * No data moves between devices.  The result equals a one-device call bit for
+ * bit.  Returns when `out` is complete; the first failing device's status and
+ * message (ctlcu_group_last_error) are reported.
+ */
+CTLCU_API int ctlcu_group_project_volume(ctlcu_group* group, const ctlcu_volume_desc* desc, const float* volume,
+                                         const ctlcu_settings* settings, const double* pmats, uint32_t n_views,
+                                         uint32_t n_modules, uint32_t channels, uint32_t rows, float* out);
+
+/* The view split of ctlcu_group_project_volume (and of bench.py's ranks):
+ * n_parts contiguous blocks whose sizes differ by at most one, the larger
+ * ones first; part i is [first[i], first[i+1]).  first holds n_parts + 1
+ * entries.  Needs no GPU. */
+CTLCU_API int ctlcu_split_views(uint32_t n_views, uint32_t n_parts, uint32_t* first);
 
 /* Wait for the context's stream; reports a deferred device-side error
  * (CTLCU_ERR_SINGULAR_GEOMETRY) raised by an earlier asynchronous call. */

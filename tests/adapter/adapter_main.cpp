@@ -5,8 +5,9 @@
 // rays_x rays_y ray_sampling upsampling interpolate"), volume.bin (float32,
 // x fastest) and pmats.bin (float64 [view][module] 3x4 row-major), then
 // configure()s, project()s and writes out.bin (float32 [view][module][row][channel]).
-// It also checks that parameter() round-trips through setParameter() and that
-// projectionFinished() fires once per view.  Test code only.
+// It also checks that parameter() round-trips through setParameter(), that
+// projectionFinished() fires once per view, and that the device lists {0, 0}
+// and {0, 0, 0} give the same bits.  Test code only.
 #include "cudaraycasterprojector.h"
 
 #include <cstdio>
@@ -91,6 +92,26 @@ int main(int argc, char** argv)
         for(uint m = 0; m < M; ++m)
             out.write(reinterpret_cast<const char*>(proj.view(v).module(m).rawData()),
                       std::streamsize(sizeof(float) * size_t(C) * R));
+
+    // the same projection spread over the device list {0, 0} and {0, 0, 0}
+    // (several contexts on one GPU, each with its contiguous block of views):
+    // identical bits to the one-device call
+    for(uint copies : { 2u, 3u })
+    {
+        s.deviceIDs.assign(copies, 0u);
+        const ProjectionData multi = projector.project(volume);
+        if(multi.nbViews() != V)
+            return 8;
+        for(uint v = 0; v < V; ++v)
+            for(uint m = 0; m < M; ++m)
+                if(std::memcmp(multi.view(v).module(m).rawData(), proj.view(v).module(m).rawData(),
+                               sizeof(float) * size_t(C) * R) != 0)
+                {
+                    std::fprintf(stderr, "deviceIDs of %u entries: view %u module %u differs\n", copies, v, m);
+                    return 9;
+                }
+    }
+    s.deviceIDs.clear();
 
     // an empty volume gives empty projections and no exception, as in the reference
     VolumeData empty({ 0, 0, 0 }, { 1, 1, 1 }, { 0, 0, 0 }, {});
