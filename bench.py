@@ -9,20 +9,28 @@ projects all 360 views.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-value    views/s over all ranks, volume resident on the device, device-side
-         P matrices and output, CUDA-event timed per step (L2 flushed between
-         steps by writing a 256 MiB buffer, outside the timed events)
+value    views/s over all ranks of the drop-in projector (FP32 storage, default
+         settings), volume resident on the device, device-side P matrices and
+         output, CUDA-event timed per step (L2 flushed between steps by writing
+         a 256 MiB buffer, outside the timed events)
 e2e      the same job through the C ABI call a CTL user makes
          (ctlcu_project_volume): host volume, host P matrices, host output,
          copies inside the timed region
 roofline the ray-casting kernel's gather bytes (samples x 8 taps x voxel bytes +
          output) per launch over its CUDA-event duration, against on-SM L1
          delivery (SMs x 128 B/clk x sampled SM clock)
+legs     (one GPU) the rest of the headline metric on the same workload: the
+         batched BF16 form (BF16 storage, 8 requests of 45 views in one
+         persistent launch replayed from a CUDA graph), the plain FP32 gather
+         loop it is compared with, the FP64 accumulator, and DRR serving
+         latency (8 x 256^3 BF16, Poisson 2000 requests/s)
 --impl reference   the reference's own kernel (raycasterprojector_interp.cl
          compiled for the CPU, oracle/_ref) on all host cores, a bounded
          sample of the same views per step
-Multi-GPU: one process per GPU (torchrun), each projecting the full job on its
-own device (weak scaling, no data-path collective).
+Multi-GPU: one process per GPU (torchrun); the 360 views are split into
+contiguous blocks by ctlcu_split_views (the view split of the multi-device
+projector), each rank projecting its block with its own copy of the volume:
+strong scaling, no data-path collective.
 """
 from __future__ import annotations
 
@@ -45,7 +53,7 @@ VOXEL = (1.0, 1.0, 1.0)
 SHAPE = (256, 256, 256)
 CHANNELS = ROWS = 512
 N_VIEWS = 360
-METRIC = "projections/s at 256^3->512^2 (plain FP32)"
+METRIC = "projections/s at 256\u00b3\u2192512\u00b2 (plain FP32 vs batched BF16); p50/p99 DRR latency"
 WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan), raySampling 0.3, trilinear"
 # DRAM bytes (read + write) of one 360-view launch of the cell loop on this
 # workload, from one ncu capture (profiles/cells_kernel_256cubed_to_512sq_dram.md),
@@ -164,6 +172,13 @@ def cpu_reference_rate(vol, P, target_s: float, threads: int):
     return n / dt, n, dt
 
 
+def bench_config(world: int, n_views: int = N_VIEWS) -> dict:
+    """The workload, identical in both arms' lines (what was run, not how it was tuned)."""
+    return {"workload": WORKLOAD, "views_per_step": n_views, "volume": "256^3 f32, 1 mm", "detector": "512x512",
+            "l2": "flushed between steps (256 MiB write outside the timed events)",
+            "parallelism": f"views split over {world} GPU(s) in contiguous blocks (ctlcu_split_views)"}
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -174,7 +189,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "unit": "projections/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
-            "config": {"workload": WORKLOAD}}
+            "config": bench_config(world)}
     if not oracle.ref_available():
         line["unavailable"] = "oracle/_ref/libctlref.so (reference kernel compiled for the CPU) is not built"
         print(json.dumps(line))
@@ -203,6 +218,24 @@ def run_reference(args):
     return 0
 
 
+def _time_steps(fn, steps, warmup, stream, flush=None):
+    """CUDA-event times (ms) of `steps` calls of fn on `stream` after `warmup`
+    untimed ones; `flush` (if given) runs between the timed calls, outside the events."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in ev:
+        if flush is not None:
+            flush()
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
 def run_ours(args):
     import torch
 
@@ -214,7 +247,13 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     n_views = args.views
-    vol, P = make_inputs(n_views)
+    vol, P_all = make_inputs(n_views)
+    # this rank's contiguous block of views: the split the multi-device projector
+    # (ctlcu_group_project_volume) uses for a device list of `world` devices
+    first = L.split_views(n_views, world)
+    v0, v1 = first[rank], first[rank + 1]
+    P = np.ascontiguousarray(P_all[v0:v1])
+    mine = v1 - v0
     settings = Settings(accum={"fp64": L.ACCUM_FP64, "kahan": L.ACCUM_KAHAN, "fp32": L.ACCUM_FP32}[args.accum],
                         storage={"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[args.storage],
                         interp_mode=L.INTERP_TEXTURE if args.interp == "texture" else L.INTERP_SOFTWARE,
@@ -227,7 +266,7 @@ def run_ours(args):
     vobj = VoxelVolume(vol, VOXEL)
     volume = ctx.volume(vobj, settings.storage)
     dP = torch.from_numpy(P).to(dev)
-    out = torch.empty((n_views, 1, ROWS, CHANNELS), dtype=torch.float32, device=dev)
+    out = torch.empty((mine, 1, ROWS, CHANNELS), dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     samples = ctx.count_samples(volume, P, CHANNELS, ROWS, settings)
     tuned = None
@@ -257,19 +296,20 @@ def run_ours(args):
         torch.cuda.synchronize()
         launches = ctx.launches() - l0
         step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = max_over_ranks(sum(step_ms), world)
+    own_ms = sum(step_ms)
+    total_ms = max_over_ranks(own_ms, world)
     ms_per_step = total_ms / args.steps
-    value = world * n_views * args.steps / (total_ms / 1e3)
+    value = n_views * args.steps / (total_ms / 1e3)
 
     # Each step is one setup launch (about 5 us for 360 views) and one projection
     # launch, timed together by the events on their stream; the step time stands
     # for the projection kernel's launch time (the setup is < 0.01% of it).
-    kernel_ms = ms_per_step
+    kernel_ms = own_ms / args.steps
 
-    # e2e through the C ABI with host buffers (pinned)
+    # e2e through the C ABI with host buffers (pinned): this rank's block
     h_vol = torch.from_numpy(vol).pin_memory()
     h_P = torch.from_numpy(P).pin_memory()
-    h_out = torch.empty((n_views, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
+    h_out = torch.empty((mine, 1, ROWS, CHANNELS), dtype=torch.float32).pin_memory()
     desc_vol = VoxelVolume(h_vol.numpy(), VOXEL)
     # as many warm-up calls as device steps: with one, the first timed calls still ran
     # up to 8% slower and the end-to-end number varied from run to run
@@ -283,12 +323,16 @@ def run_ours(args):
         ctx.project_volume(desc_vol, h_P.numpy(), CHANNELS, ROWS, settings, out=h_out.numpy())
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = max_over_ranks(sum(e2e_ms), world)
-    e2e_value = world * n_views * len(e2e_ms) / (e2e_total / 1e3)
+    e2e_value = n_views * len(e2e_ms) / (e2e_total / 1e3)
     clk = clocks.stop()
+
+    legs = None
+    if world == 1 and not args.headline_only:
+        legs = run_legs(args, ctx, vobj, volume, P, flush, stream, value)
 
     if rank == 0:
         b = 4 if settings.storage == L.F32 else 2
-        alg_bytes = samples * 8 * b + 4 * n_views * ROWS * CHANNELS
+        alg_bytes = samples * 8 * b + 4 * mine * ROWS * CHANNELS
         props = torch.cuda.get_device_properties(dev)
         sms = props.multi_processor_count
         mhz = clk.get("sm_mhz") or 1965.0
@@ -296,29 +340,29 @@ def run_ours(args):
         achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
         loop = ran.kernel
         shape = ran.launch_shape()
-        traffic = (CELLS_TRAFFIC_BYTES if loop == L.KERNEL_CELLS and n_views == N_VIEWS and
+        traffic = (CELLS_TRAFFIC_BYTES if loop == L.KERNEL_CELLS and mine == N_VIEWS and
                    settings.storage == L.F32 and settings.interp_mode == L.INTERP_SOFTWARE and
                    args.accum == CELLS_TRAFFIC_ACCUM and tuple(shape.values()) == CELLS_TRAFFIC_SHAPE else None)
         line = {
             "metric": METRIC, "value": value, "unit": "projections/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": {L.F32: "f32", L.BF16: "bf16", L.F16: "f16"}[settings.storage] + "-storage/f32-interp/"
                      + args.accum + "-accum",
             "data": "synthetic (seeded ellipsoid phantom, seeded jittered geometry)",
-            "config": {"workload": WORKLOAD, "views_per_step": n_views, "volume": "256^3", "detector": "512x512",
-                       "interp": args.interp, "kernel": args.kernel,
-                       "loop": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs",
-                                L.KERNEL_GATHER: "gather"}.get(loop, "auto"),
-                       "launch_shape": shape,
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"views replicated per GPU x{world}"},
+            "config": bench_config(world, n_views),
+            "run": {"storage": {L.F32: "f32", L.BF16: "bf16", L.F16: "f16"}[settings.storage],
+                    "accum": args.accum, "interp": args.interp, "kernel": args.kernel,
+                    "loop": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs",
+                             L.KERNEL_GATHER: "gather"}.get(loop, "auto"),
+                    "launch_shape": shape, "views_of_rank0": [v0, v1]},
+            "vs_baseline_note": "no published number for this metric (BASELINE.md section 1)",
             "samples_per_step": samples,
-            "gsamples_per_s": samples * world * args.steps / (total_ms / 1e3) / 1e9,
+            "gsamples_per_s": samples * args.steps / (own_ms / 1e3) / 1e9,
             "e2e": {"value": e2e_value, "unit": "projections/s",
                     "h2d_bytes_per_step": int(vol.nbytes + P.nbytes),
                     "d2h_bytes_per_step": int(h_out.numel() * 4),
-                    "path": "ctlcu_project_volume, pinned host buffers"},
+                    "path": "ctlcu_project_volume, pinned host buffers (per rank: its block of views)"},
             "gpu_launches": int(launches),
             "autotune": None if tuned is None else {
                 "chosen": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs", L.KERNEL_GATHER: "gather"}[tuned[0]],
@@ -335,10 +379,12 @@ def run_ours(args):
                          "dram_frac_of_hbm": traffic / (kernel_ms / 1e3) / 1e9 / hbm_peak() if traffic else None},
             "clocks": clk,
         }
+        if legs is not None:
+            line["legs"] = legs
         if world == 1 and not args.no_cpu_baseline:
             import oracle
             if oracle.ref_available():
-                rate, n, dt = cpu_reference_rate(vol, P, args.cpu_seconds, os.cpu_count() or 1)
+                rate, n, dt = cpu_reference_rate(vol, P_all, args.cpu_seconds, os.cpu_count() or 1)
                 line["cpu_baseline"] = {"value": rate, "unit": "projections/s", "cores": os.cpu_count(),
                                         "kind": "reference",
                                         "sample": f"{n} of {N_VIEWS} views evenly spaced, {dt:.1f} s"}
@@ -346,12 +392,12 @@ def run_ours(args):
             # raycasterprojectorcpu.cpp:132-285), as the oracle restates it, timed once beside it
             threads = os.cpu_count() or 1
             t0 = time.perf_counter()
-            oracle.project_fp64(vol, VOXEL, P[:1], CHANNELS, ROWS, threads=threads)
+            oracle.project_fp64(vol, VOXEL, P_all[:1], CHANNELS, ROWS, threads=threads)
             t1 = time.perf_counter() - t0
             n = int(max(1, min(N_VIEWS, round(0.5 * args.cpu_seconds / max(t1, 1e-3)))))
             idx = np.linspace(0, N_VIEWS - 1, n).round().astype(int)
             t0 = time.perf_counter()
-            oracle.project_fp64(vol, VOXEL, P[idx], CHANNELS, ROWS, threads=threads)
+            oracle.project_fp64(vol, VOXEL, P_all[idx], CHANNELS, ROWS, threads=threads)
             dt = time.perf_counter() - t0
             line["cpu_fp64_twin"] = {"value": n / dt, "unit": "projections/s", "cores": threads, "kind": "port",
                                      "sample": f"{n} of {N_VIEWS} views evenly spaced, {dt:.1f} s"}
@@ -362,6 +408,56 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def run_legs(args, ctx, vobj, volume, P, flush, stream, value_fp32):
+    """The rest of the headline metric on one GPU: the FP64 accumulator, the
+    plain FP32 gather loop, the batched BF16 form and DRR serving latency."""
+    import torch
+
+    from ctl_b200 import _lib as L
+    from ctl_b200.projector import Settings
+    V = P.shape[0]
+    dP = torch.from_numpy(P).cuda()
+    out = torch.empty((V, 1, ROWS, CHANNELS), dtype=torch.float32, device="cuda")
+    steps = max(3, args.steps // 2)
+    legs = {}
+
+    def rate(ms):
+        return V / (statistics.mean(ms) / 1e3)
+
+    # the reference kernel's own accumulator type (FP64), same loop and shape
+    s64 = Settings(accum=L.ACCUM_FP64)
+    ms = _time_steps(lambda: ctx.project(volume, dP, CHANNELS, ROWS, s64, out=out, stream=ctx.stream), steps,
+                     args.warmup, stream, flush.zero_)
+    legs["accum_fp64"] = {"value": rate(ms), "unit": "projections/s", "ms_per_step": statistics.mean(ms),
+                          "what": "FP32 storage, cell loop, FP64 accumulator"}
+    # the plain FP32 CUDA projector: eight scalar loads per sample from the padded voxels
+    sg = Settings(kernel=L.KERNEL_GATHER)
+    ms = _time_steps(lambda: ctx.project(volume, dP, CHANNELS, ROWS, sg, out=out, stream=ctx.stream), steps,
+                     args.warmup, stream, flush.zero_)
+    plain = rate(ms)
+    legs["plain_gather_fp32"] = {"value": plain, "unit": "projections/s", "ms_per_step": statistics.mean(ms),
+                                 "what": "FP32 storage, gather loop (8 scalar loads per sample), Kahan accumulator"}
+    # the batched BF16 form: BF16 storage, 8 requests of 45 views (clients of one volume)
+    # in one persistent launch, replayed from a CUDA graph (ctlcu_plan_launch)
+    vb = ctx.volume(vobj, L.BF16)
+    ctx.autotune(vb, P, CHANNELS, ROWS, Settings())
+    parts = L.split_views(V, 8)
+    reqs = [(vb, dP[parts[i]:parts[i + 1]], out[parts[i]:parts[i + 1]]) for i in range(8)]
+    plan = ctx.plan(reqs, Settings())
+    ms = _time_steps(lambda: plan.launch(ctx.stream), args.steps, args.warmup, stream, flush.zero_)
+    batched = rate(ms)
+    legs["batched_bf16"] = {"value": batched, "unit": "projections/s", "ms_per_step": statistics.mean(ms),
+                            "what": "BF16 storage, 8 requests x 45 views, one persistent launch per step "
+                                    "replayed from a CUDA graph (ctlcu_plan_launch)",
+                            "vs_plain_gather_fp32": batched / plain, "vs_drop_in_fp32": batched / value_fp32}
+    plan.close()
+    del reqs
+    vb.release()
+    torch.cuda.synchronize()
+    legs["drr"] = drr_measurements(ctx, args, sweep=False)
+    return legs
 
 
 # ---- the other configurations (extra lines; the headline is the 256^3 -> 512^2 one above) ------
@@ -850,53 +946,77 @@ def run_c4(args):
     ctx.close()
 
 
-def run_c5(args):
-    """DRR serving: capacity, then latency percentiles at 2000 requests/s offered."""
-    import torch
-
+def drr_measurements(ctx, args, sweep: bool = True) -> dict:
+    """DRR serving on 8 resident 256^3 BF16 volumes: capacity, latency at 2000
+    requests/s offered, the highest offered rate whose p99 stays under 5 ms, and
+    the sample count the 2000/s stream asks for."""
     from ctl_b200 import _lib as L
     from ctl_b200 import workloads as W
-    from ctl_b200.projector import Context, Settings, VoxelVolume
+    from ctl_b200.projector import Settings, VoxelVolume
     from ctl_b200.serving import DRRServer, poisson_requests
-    ctx = Context(0)
     vols = [ctx.volume(VoxelVolume(v, (1.0, 1.0, 1.0)), L.BF16) for v in W.c5_volumes()]
     kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
-                                 "pairs": L.KERNEL_PAIRS}[args.kernel]
+              "pairs": L.KERNEL_PAIRS}[args.kernel]
+    settings = Settings(kernel=kernel)
     # 2 streams and batches of at most 24 views: a batch's persistent launch holds the SMs
     # until it is done, so bounding its views bounds how long later requests wait behind it
-    # (a sweep of 1-3 streams and 24-256-view caps gave the lowest p99 at 500-1300 req/s
-    # for this setting, at the same capacity)
-    server = DRRServer(ctx, vols, 256, 256, Settings(kernel=kernel), streams=2, max_batch=256,
+    server = DRRServer(ctx, vols, 256, 256, settings, streams=2, max_batch=256,
                        budget_bytes=40 * 10**9, max_batch_views=24)
     base = W.c5_base_view()
     server.warm_up(typical_pmats=np.repeat(base[None], 8, axis=0) if kernel == L.KERNEL_AUTO else None)
     # capacity: all requests offered at once.  The first run of this size also grows the
-    # device allocators (outputs and batch descriptors of 2000 requests) and ran up to 30%
-    # slower, so one untimed run comes first; then three runs, the median reported with the spread
+    # device allocators and ran up to 30% slower, so one untimed run comes first
     server.run(poisson_requests(1e7, 2000, len(vols), base, seed=49))
-    caps = [server.run(poisson_requests(1e7, 2000, len(vols), base, seed=50 + 100 * i)).summary() for i in range(3)]
+    n_cap = 3 if sweep else 1
+    caps = [server.run(poisson_requests(1e7, 2000, len(vols), base, seed=50 + 100 * i)).summary()
+            for i in range(n_cap)]
     caps.sort(key=lambda c: c["throughput_req_s"])
-    cap = dict(caps[1], runs_req_s=[c["throughput_req_s"] for c in caps])
+    cap = dict(caps[len(caps) // 2], runs_req_s=[c["throughput_req_s"] for c in caps])
     rate = 2000.0
-    n = int(rate * args.serve_seconds)
-    at = server.run(poisson_requests(rate, n, len(vols), base, seed=51)).summary()
+    stream_2000 = poisson_requests(rate, int(rate * args.serve_seconds), len(vols), base, seed=51)
+    at = server.run(stream_2000).summary()
+    # the work the 2000/s stream asks for: exact reference-scheme samples of its requests
+    samples = 0
+    for k, v in enumerate(vols):
+        mats = [r.pmats for r in stream_2000 if r.volume == k]
+        if mats:
+            samples += ctx.count_samples(v, np.concatenate(mats), 256, 256, settings)
+    n_req = len(stream_2000)
+    n_views = sum(int(r.pmats.shape[0]) for r in stream_2000)
+    span_s = n_req / rate
     # offered-rate sweep: the highest rate whose p99 stays under 5 ms
-    sweep = []
-    for frac in (0.2, 0.35, 0.5, 0.65, 0.8):
+    fracs = (0.2, 0.35, 0.5, 0.65, 0.8) if sweep else (0.35, 0.5, 0.65)
+    points = []
+    for frac in fracs:
         r_off = frac * cap["throughput_req_s"]
-        s = server.run(poisson_requests(r_off, max(200, int(r_off * args.serve_seconds)), len(vols), base,
-                                        seed=52 + int(100 * frac))).summary()
-        sweep.append(dict(s, offered_req_s=r_off))
-    ok = [s["offered_req_s"] for s in sweep if s["p99_ms"] < 5.0]
-    _line("p99 DRR latency at 2000 requests/s (8 x 256^3 BF16, 1-16 views of 256^2)", at["p99_ms"], "ms",
-          at["p50_ms"], args,
-          {"workload": "8 resident 256^3 BF16 volumes; Poisson 2000/s; 1-16 perturbed views of 256^2 @1.2 mm",
-           "budget_bytes": 40 * 10**9}, higher_is_better=False, serving_at_2000=at, capacity=cap,
-          sweep=sweep, max_rate_p99_under_5ms=max(ok) if ok else None,
-          autotuned=[t[0] for t in getattr(server, "tuned", [])],
-          launch_shapes=[ctx.tuned_settings(v, 1, 256, 256, Settings(kernel=kernel)).launch_shape() for v in vols])
+        sm = server.run(poisson_requests(r_off, max(200, int(r_off * args.serve_seconds)), len(vols), base,
+                                         seed=52 + int(100 * frac))).summary()
+        points.append(dict(sm, offered_req_s=r_off))
+    ok = [q["offered_req_s"] for q in points if q["p99_ms"] < 5.0]
+    res = {"unit": "ms", "offered_req_s": rate, "p50_ms": at["p50_ms"], "p95_ms": at["p95_ms"],
+           "p99_ms": at["p99_ms"], "achieved_req_s": at["throughput_req_s"],
+           "mean_requests_per_batch": at["mean_requests_per_batch"], "at_2000": at, "capacity": cap,
+           "sweep": points, "max_rate_p99_under_5ms": max(ok) if ok else None,
+           "work_at_2000": {"requests": n_req, "views": n_views, "samples": samples,
+                            "samples_per_view": samples / max(n_views, 1),
+                            "samples_per_s_needed": samples / span_s,
+                            "samples_per_s_at_capacity": samples / n_views * cap["throughput_views_s"]},
+           "workload": "8 resident 256^3 BF16 volumes; Poisson 2000/s; 1-16 perturbed views of 256^2 @1.2 mm; "
+                       "40 GB budget; 2 streams, <= 24 views per batch",
+           "launch_shapes": [ctx.tuned_settings(v, 1, 256, 256, settings).launch_shape() for v in vols]}
     for v in vols:
         v.release()
+    return res
+
+
+def run_c5(args):
+    """DRR serving: capacity, then latency percentiles at 2000 requests/s offered."""
+    from ctl_b200.projector import Context
+    ctx = Context(0)
+    d = drr_measurements(ctx, args, sweep=True)
+    _line("p99 DRR latency at 2000 requests/s (8 x 256^3 BF16, 1-16 views of 256^2)", d["p99_ms"], "ms",
+          d["p50_ms"], args, {"workload": d["workload"], "budget_bytes": 40 * 10**9}, higher_is_better=False,
+          serving=d)
     ctx.close()
 
 
@@ -926,6 +1046,8 @@ def main():
                     default="c2",
                     help="c2 (default) is the headline; the others print extra lines")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the one-GPU legs (FP64 accumulator, gather, batched BF16, DRR serving)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -145,6 +145,10 @@ __host__ __device__ __forceinline__ uint32_t cell_linear(uint32_t ix, uint32_t i
                             // 3: texture fetch on change
 #endif
 
+#ifndef CTLCU_CELL_PAIRED
+#define CTLCU_CELL_PAIRED 0  // 1: the cell loop evaluates two consecutive samples per packed f32x2 operation
+#endif
+
 #ifndef CTLCU_CELL_PREFETCH
 #define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
 #endif
@@ -225,7 +229,8 @@ struct BatchSetup {
 };
 
 // One request of a batched projection (device array): its launch arguments
-// (geom pointing at its ViewGeom entries) and its range of work items.
+// (geom pointing at its ViewGeom entries) and its range of work items (block
+// tiles of the single-request launch).
 struct BatchReq {
     ProjectArgs a;
     uint32_t first_item;  // first work item (block) of this request
@@ -236,8 +241,10 @@ struct BatchReq {
 cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t total, ViewGeom* geom,
                                int* flags, cudaStream_t s);
 // Persistent launch (Mode::Cells or Mode::Pairs) over all work items of a
-// batch, every request with the launch shape `shape` (block size and unroll);
-// `counter` must be zero at launch.  Returns the grid size in *blocks.
+// batch (total_items block tiles, each block / 32 warp patches, dealt out to
+// warps one patch at a time), every request with the launch shape `shape`
+// (block size and unroll); `counter` must be zero at launch.  Returns the
+// grid size in *blocks.
 cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
                          const LaunchShape& shape, unsigned int* counter, int* blocks, cudaStream_t s);
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,

@@ -386,11 +386,98 @@ __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const cha
     return fmaf(hz, g.y, g.x);
 }
 
+#if CTLCU_CELL_PAIRED
+// The interpolant of the cached cell at offsets (hx, hy, hz) from its centre,
+// loading the cell first if `idx` differs from the cached one (see cell_sample).
+__device__ __forceinline__ float cell_eval(const char* __restrict__ cells, uint32_t idx, float hx, float hy,
+                                           float hz, CellCache& cc)
+{
+    {
+        const char* p = cells + (size_t)idx * kCellBytes;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %8, %9;\n\t"
+                     "@p ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%10];\n\t}"
+                     : "+f"(cc.c0), "+f"(cc.c1), "+f"(cc.c2), "+f"(cc.c3), "+f"(cc.c4), "+f"(cc.c5),
+                       "+f"(cc.c6), "+f"(cc.c7)
+                     : "r"(idx), "r"(cc.idx), "l"(p));
+        cc.idx = idx;
+    }
+    const float2 hx2 = make_float2(hx, hx);
+    const float2 ea = __ffma2_rn(hx2, make_float2(cc.c2, cc.c3), make_float2(cc.c0, cc.c1));
+    const float2 eb = __ffma2_rn(hx2, make_float2(cc.c6, cc.c7), make_float2(cc.c4, cc.c5));
+    const float2 g = __ffma2_rn(make_float2(hy, hy), eb, ea);
+    return fmaf(hz, g.y, g.x);
+}
+
+// Two consecutive samples (steps k and k + 1, the lanes of kk) of cell_sample
+// at once: each packed f32x2 operation holds one axis of both samples, so the
+// position, rounding and offset arithmetic of the z axis shares the packed
+// instructions of x and y.  Per sample the operations and their rounding are
+// those of cell_sample, so the values are identical.
+__device__ __forceinline__ float2 cell_sample_pair(const char* __restrict__ cells, float2 kk, const CellFrame& fr,
+                                                   float2 dx2, float2 dy2, float2 dz2, uint32_t sy, uint32_t sz,
+                                                   uint32_t cmax, CellCache& cc)
+{
+    const float2 none2 = make_float2(-1.0f, -1.0f);
+    const float2 mx2 = make_float2(fr.mxy.x, fr.mxy.x), my2 = make_float2(fr.mxy.y, fr.mxy.y);
+    const float2 mz2 = make_float2(fr.mz, fr.mz);
+    const float2 vx = __ffma2_rn(kk, dx2, make_float2(fr.bxy.x, fr.bxy.x));
+    const float2 vy = __ffma2_rn(kk, dy2, make_float2(fr.bxy.y, fr.bxy.y));
+    const float2 vz = __ffma2_rn(kk, dz2, make_float2(fr.bz, fr.bz));
+    const float2 tx = __fadd2_rn(vx, mx2), ty = __fadd2_rn(vy, my2), tz = __fadd2_rn(vz, mz2);
+    const float2 hx = __ffma2_rn(__ffma2_rn(mx2, none2, tx), none2, vx);  // v - (t - m)
+    const float2 hy = __ffma2_rn(__ffma2_rn(my2, none2, ty), none2, vy);
+    const float2 hz = __ffma2_rn(__ffma2_rn(mz2, none2, tz), none2, vz);
+    const uint32_t i0 = min(cell_linear(__float_as_uint(tx.x), __float_as_uint(ty.x), __float_as_uint(tz.x), sy, sz),
+                            cmax);
+    const uint32_t i1 = min(cell_linear(__float_as_uint(tx.y), __float_as_uint(ty.y), __float_as_uint(tz.y), sy, sz),
+                            cmax);
+    const float f0 = cell_eval(cells, i0, hx.x, hy.x, hz.x, cc);
+    const float f1 = cell_eval(cells, i1, hx.y, hy.y, hz.y, cc);
+    return make_float2(f0, f1);
+}
+#endif
+
 // Sample loop over the coefficient cells, U samples per partial sum (FP32)
 // handed to the accumulator.
 template <Accum ACC, int U>
 __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
+#if CTLCU_CELL_PAIRED
+    const char* __restrict__ cells = static_cast<const char*>(a.cells);
+    const CellFrame fr = cell_frame(r);
+    const float2 dx2 = make_float2((float)r.step[0], (float)r.step[0]);
+    const float2 dy2 = make_float2((float)r.step[1], (float)r.step[1]);
+    const float2 dz2 = make_float2((float)r.step[2], (float)r.step[2]);
+    const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
+    const float2 two2 = make_float2(2.0f, 2.0f);
+    float2 kk = make_float2(0.0f, 1.0f);  // steps k and k + 1
+    CellCache cc;
+    int k = 0;
+    for (; k + U <= r.n; k += U) {
+        float part = 0.0f;
+#pragma unroll
+        for (int j = 0; j < U; j += 2) {
+            const float2 f = cell_sample_pair(cells, kk, fr, dx2, dy2, dz2, sy, sz, cmax, cc);
+            part += f.x;
+            part += f.y;
+            kk = __fadd2_rn(kk, two2);
+        }
+        acc.add(part);
+    }
+    if (k < r.n) {
+        // the last r.n - k < U samples, pairwise; a lone last sample takes the
+        // first value of a pair whose second step lies beyond the ray (its cell
+        // index is clamped like any other, its value unused)
+        for (; k + 1 < r.n; k += 2) {
+            const float2 f = cell_sample_pair(cells, kk, fr, dx2, dy2, dz2, sy, sz, cmax, cc);
+            acc.add(f.x);
+            acc.add(f.y);
+            kk = __fadd2_rn(kk, two2);
+        }
+        if (k < r.n)
+            acc.add(cell_sample_pair(cells, kk, fr, dx2, dy2, dz2, sy, sz, cmax, cc).x);
+    }
+#else
     const char* __restrict__ cells = static_cast<const char*>(a.cells);
     const CellFrame fr = cell_frame(r);
     const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
@@ -429,6 +516,7 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
     }
 #if CTLCU_CELL_PREFETCH > 0
     asm volatile("cp.async.wait_all;" ::: "memory");
+#endif
 #endif
 }
 
@@ -596,54 +684,49 @@ __global__ void __maxnreg__(CTLCU_CELL_MAXREG) cells_kernel(const ProjectArgs a)
     cells_item<M, ACC, U>(a, blockIdx.x, threadIdx.x);
 }
 
-// Persistent batch kernel: blocks take work items in order from `counter`
-// until all requests' items are done.  Work items of one request are its
-// blocks in the order of the single-request launch, so blocks running at the
-// same time work on neighbouring views of one volume.
+// Persistent batch kernel with warp-granular work: every warp takes one warp
+// patch (32 rays: patch w of block tile b of a request) at a time from
+// `counter` and runs it, with no barrier between the warps of a block.  A warp
+// whose rays are short (a tile edge, rays that miss the volume) takes the next
+// patch at once instead of waiting for the longest ray of its tile, so the SMs
+// stay busy to the end of the batch.  Warp items run in the order of the
+// single-request launch's blocks and, within a block tile, its warps: warps that
+// run at the same time work on neighbouring patches and views of one volume.
 //
-// Per item the block's bookkeeping stays off the critical path: thread 0 takes the
-// index of its next item from the counter while the current one runs; a block's
-// items only grow, so the request of an item is found by scanning forward from the
-// previous one; and the request's launch arguments are copied to shared memory
-// only when the request changes.
+// Per warp, the request of its item is found by scanning forward from the
+// previous one (a warp's items only grow), and the request's launch arguments
+// are copied into the warp's own slot of shared memory only when the request
+// changes.
 template <Mode M, Accum ACC, int U>
 __global__ void __maxnreg__(CTLCU_CELL_MAXREG)
-    batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total, unsigned int* counter)
+    batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total_warp_items,
+                       uint32_t wpb_shift, unsigned int* counter)
 {
-    __shared__ ProjectArgs sa;
-    __shared__ uint32_t s_req, s_local;
+    extern __shared__ __align__(16) unsigned char s_raw[];  // one ProjectArgs per warp
     static_assert(sizeof(ProjectArgs) % 4 == 0, "word copy");
-    uint32_t next = 0, req = 0;  // thread 0: the item to run next and the request of the last one
-    if (threadIdx.x == 0)
-        next = atomicAdd(counter, 1u);
-    uint32_t loaded = 0xffffffffu;  // request whose arguments `sa` holds (the same in every thread)
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    ProjectArgs& sa = reinterpret_cast<ProjectArgs*>(s_raw)[warp];
+    uint32_t req = 0, loaded = 0xffffffffu;  // the same in every lane of the warp
     for (;;) {
-        if (threadIdx.x == 0) {
-            const uint32_t it = next;
-            if (it < total) {
-                while (req + 1 < n_reqs && reqs[req + 1].first_item <= it)
-                    ++req;  // the last request with first_item <= it
-                s_local = it - reqs[req].first_item;
-                s_req = req;
-                next = atomicAdd(counter, 1u);
-            } else {
-                s_req = 0xffffffffu;
-            }
-        }
-        __syncthreads();
-        const uint32_t r = s_req;
-        if (r == 0xffffffffu)
+        uint32_t it = 0;
+        if (lane == 0)
+            it = atomicAdd(counter, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= total_warp_items)
             return;
-        if (r != loaded) {  // uniform: every thread read the same s_req
-            const uint32_t* src = reinterpret_cast<const uint32_t*>(&reqs[r].a);
+        const uint32_t item = it >> wpb_shift, w = it & ((1u << wpb_shift) - 1u);
+        while (req + 1 < n_reqs && reqs[req + 1].first_item <= item)
+            ++req;  // the last request with first_item <= item
+        if (req != loaded) {
+            __syncwarp();  // every lane is done with the previous request's arguments
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&reqs[req].a);
             uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
-            for (uint32_t i = threadIdx.x; i < sizeof(ProjectArgs) / 4; i += blockDim.x)
+            for (uint32_t i = lane; i < sizeof(ProjectArgs) / 4; i += 32)
                 dst[i] = src[i];
-            loaded = r;
-            __syncthreads();
+            __syncwarp();
+            loaded = req;
         }
-        cells_item<M, ACC, U>(sa, s_local, threadIdx.x);
-        __syncthreads();
+        cells_item<M, ACC, U>(sa, item - reqs[req].first_item, (w << 5) + lane);
     }
 }
 
@@ -700,6 +783,9 @@ __global__ void __launch_bounds__(kMaxBlock) count_kernel(const ProjectArgs a)
     if ((threadIdx.x & 31u) == 0 && n)
         atomicAdd(a.counter, n);
 }
+
+// log2 of the warps in a block of 128, 256 or 512 threads.
+uint32_t log2_block_warps(uint32_t block) { return block == 128 ? 2u : (block == 256 ? 3u : 4u); }
 
 // The launch's block size must be one the pixel mapping was built for.
 bool block_ok(const ProjectArgs& a)
@@ -771,19 +857,27 @@ template <Mode M, Accum ACC, int U>
 cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t total, uint32_t block,
                                unsigned int* counter, int* blocks, cudaStream_t s)
 {
+    // warp items: each block tile of `block` rays is block / 32 warp patches
+    const uint32_t wpb = block / 32u, wpb_shift = log2_block_warps(block);
+    const uint64_t warp_items = (uint64_t)total * wpb;
+    // the counter runs past the end by one per warp of the grid: keep it clear of wrapping
+    if (warp_items > 0xffffffffull - (1ull << 20))
+        return cudaErrorInvalidValue;
+    const size_t smem = sizeof(ProjectArgs) * wpb;
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<M, ACC, U>, (int)block, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cells_kernel<M, ACC, U>, (int)block, smem);
     if (e != cudaSuccess)
         return e;
     uint64_t grid = (uint64_t)sms * (uint64_t)(per_sm > 0 ? per_sm : 1);
     if (grid > total)
         grid = total;
     *blocks = (int)grid;
-    batch_cells_kernel<M, ACC, U><<<(unsigned)grid, block, 0, s>>>(reqs, n_reqs, total, counter);
+    batch_cells_kernel<M, ACC, U><<<(unsigned)grid, block, smem, s>>>(reqs, n_reqs, (uint32_t)warp_items, wpb_shift,
+                                                                      counter);
     return cudaGetLastError();
 }
 

@@ -12,7 +12,9 @@ the device and requests are batched as they arrive:
 * batching: whenever one of `streams` CUDA streams is free, every queued
   request (up to `max_batch`) goes into one persistent launch on it
   (ctlcu_project_batch), so requests that arrive while others run are picked
-  up as soon as a stream frees and their work overlaps on the device;
+  up as soon as a stream frees and their work overlaps on the device; the
+  batch's matrices go through the stream's pinned staging buffer with a
+  non-blocking copy, and its outputs are one allocation sliced per request;
 * timing: latency is arrival (host clock) to the end of the request's batch
   on the device (CUDA event), with the device clock tied to the host clock
   at start.
@@ -94,6 +96,12 @@ class DRRServer:
         self.budget_bytes = budget_bytes
         if self._free_budget() <= 0:
             raise ValueError("the resident volumes alone exceed the memory budget")
+        # per stream: pinned host staging for a batch's projection matrices and the
+        # device buffer they are copied into, grown on demand.  A stream takes its
+        # next batch only after the previous one's end event, so a batch never
+        # overwrites matrices that are still being copied or read.
+        self._pin = [None] * streams
+        self._dev = [None] * streams
 
     def _free_budget(self) -> int:
         """Budget left for requests after the resident volumes (with their cell arrays)."""
@@ -125,6 +133,26 @@ class DRRServer:
             self.ctx.project_batch([(v, dP, out)], self.settings, stream=stream)
         torch.cuda.synchronize()
         self.ctx.sync()
+
+    def _stage(self, i: int, batch: Sequence[DRRRequest]):
+        """The batch's matrices gathered into stream i's pinned staging buffer and
+        copied to its device buffer without blocking the host (on the current
+        stream, which is stream i): an (n_view_modules, 12) float64 device view."""
+        torch = self.torch
+        n = sum(int(r.pmats.shape[0] * r.pmats.shape[1]) for r in batch)
+        if self._pin[i] is None or self._pin[i].shape[0] < n:
+            cap = max(n, 256)
+            self._pin[i] = torch.empty((cap, 12), dtype=torch.float64).pin_memory()
+            self._dev[i] = torch.empty((cap, 12), dtype=torch.float64, device="cuda")
+        host = self._pin[i].numpy()
+        at = 0
+        for r in batch:
+            k = int(r.pmats.shape[0] * r.pmats.shape[1])
+            host[at: at + k] = r.pmats.reshape(k, 12)
+            at += k
+        dev = self._dev[i][:n]
+        dev.copy_(self._pin[i][:n], non_blocking=True)
+        return dev
 
     def run(self, requests: Sequence[DRRRequest]) -> ServeStats:
         torch = self.torch
@@ -189,15 +217,16 @@ class DRRServer:
                             take += 1
                     batch, queue = queue[:take], queue[take:]
                     with torch.cuda.stream(s):
-                        # one host-to-device copy for the whole batch's matrices
-                        allP = torch.from_numpy(np.concatenate([r.pmats.reshape(-1, 12) for r in batch]))
-                        allP = allP.to("cuda", non_blocking=False)
+                        allP = self._stage(i, batch)
+                        # one output allocation per batch; each request keeps its slice
+                        n_vm = allP.shape[0]
+                        outs = torch.empty((n_vm, self.rows, self.channels), device="cuda")
                         items, at = [], 0
                         for r in batch:
                             V, M = r.pmats.shape[:2]
                             dP = allP[at: at + V * M].view(V, M, 3, 4)
+                            r.out = outs[at: at + V * M].view(V, M, self.rows, self.channels)
                             at += V * M
-                            r.out = torch.empty((V, M, self.rows, self.channels), device="cuda")
                             items.append((self.volumes[r.volume], dP, r.out))
                         self.ctx.project_batch(items, self.settings, stream=torch_stream_handle(s))
                         ev = torch.cuda.Event(enable_timing=True)
