@@ -25,6 +25,15 @@ def test_view_split_is_contiguous_balanced_and_complete(n_views, n_parts):
     assert list(sizes) == sorted(sizes, reverse=True)
 
 
+def test_rank_shards_follow_the_library_split():
+    """bench.py's ranks and ctl_b200.sharding take the blocks ctlcu_split_views gives."""
+    from ctl_b200.sharding import shard_views
+    for n_views, world in [(360, 8), (361, 3), (90, 7), (5, 8), (1440, 6)]:
+        first = L.split_views(n_views, world)
+        assert [shard_views(n_views, world, r) for r in range(world)] == \
+            [(first[r], first[r + 1]) for r in range(world)]
+
+
 def test_view_split_refuses_no_parts():
     lib = L.load()
     import ctypes as C

@@ -79,9 +79,9 @@ def test_projector_reuses_the_volume_across_calls():
     a = p.project(VoxelVolume(vol, (2.0, 2.0, 2.0))).numpy()
     b = p.project(VoxelVolume(vol, (2.0, 2.0, 2.0))).numpy()
     np.testing.assert_array_equal(a, b)
-    st = p.context().volume_cache_stats()
+    st = p.context.volume_cache_stats()
     assert st["hits"] >= 1 and st["resident"] >= 1
     p.settings().volume_cache = 0
     c = p.project(VoxelVolume(vol, (2.0, 2.0, 2.0))).numpy()
     np.testing.assert_array_equal(a, c)
-    assert p.context().volume_cache_stats()["resident"] == 0
+    assert p.context.volume_cache_stats()["resident"] == 0

@@ -8,6 +8,8 @@ array.  The file sorts last, so a run that stops at the first failure has run
 every other test before it; it also passes alone in a fresh process, where its
 first call looks up the array's device address.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -65,11 +67,21 @@ def test_noalloc_rejects_what_it_cannot_serve(job):
     with pytest.raises(L.CtlcuError) as e:
         ctx.project_noalloc(vol, dP, out, Settings(kernel=L.KERNEL_GATHER))
     assert e.value.status == L.ERR_INVALID_ARGUMENT and "scratch limit" in str(e.value)
-    # host buffers would need staging memory
+    # host buffers would need staging memory: the binding refuses them before the
+    # call, and the C ABI refuses them too
     P = np.ascontiguousarray(j.pmats[:2])
-    with pytest.raises(L.CtlcuError) as e:
-        ctx.project_noalloc(vol, P, np.zeros((2, 1, R, C_), np.float32), Settings(kernel=L.KERNEL_GATHER))
-    assert e.value.status == L.ERR_INVALID_ARGUMENT
+    host_out = np.zeros((2, 1, R, C_), np.float32)
+    with pytest.raises(ValueError):
+        ctx.project_noalloc(vol, P, host_out, Settings(kernel=L.KERNEL_GATHER))
+    st = Settings(kernel=L.KERNEL_GATHER).to_c()
+    rc = ctx.lib.ctlcu_project_noalloc(ctx.h, vol.handle, ctypes.byref(st), ctypes.c_void_p(P.ctypes.data), 2, 1,
+                                       C_, R, ctypes.c_void_p(host_out.ctypes.data), None)
+    assert rc == L.ERR_INVALID_ARGUMENT
+    # buffers the kernel would index past: float32 matrices, an output of other views
+    with pytest.raises(ValueError):
+        ctx.project_noalloc(vol, torch.from_numpy(P).float().cuda(), torch.empty((2, 1, R, C_), device="cuda"))
+    with pytest.raises(ValueError):
+        ctx.project_noalloc(vol, torch.from_numpy(P).cuda(), torch.empty((3, 1, R, C_), device="cuda"))
     # a derived array that no earlier call built: the mean-voxel volume
     dP2 = torch.from_numpy(P).cuda()
     out2 = torch.empty((2, 1, R, C_), device="cuda")
