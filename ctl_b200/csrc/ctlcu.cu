@@ -1443,9 +1443,131 @@ struct ctlcu_plan {
     std::vector<uint64_t> volumes;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    std::vector<ctlcu_request> fallback;  // requests when the batch is not persistent
     ctlcu_settings settings{};
+    int form = CTLCU_PLAN_PERSISTENT;   // the form the graph holds
+    float ms[2] = { 0.0f, 0.0f };       // replay time of each form, measured at creation
+    uint64_t launches_per_replay = 2;
 };
+
+namespace {
+
+// The batch as one grid launch per request (the single-request kernel, whose
+// arguments sit in the constant bank), dealt out longest first over `branch`
+// streams that fork from and join back into `st`: launches of different
+// requests overlap, so one fills the SMs that another's last wave leaves idle.
+int enqueue_batch_grids(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, cudaStream_t st,
+                        const std::vector<cudaStream_t>& branch, const std::vector<cudaEvent_t>& ev)
+{
+    const uint32_t n = (uint32_t)bp.reqs.size();
+    CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
+    CU_TRY(ctx, cudaEventRecord(ev[0], st));
+    for (cudaStream_t b : branch)
+        CU_TRY(ctx, cudaStreamWaitEvent(b, ev[0], 0));
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i)
+        order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return bp.reqs[x].items > bp.reqs[y].items; });
+    std::vector<uint64_t> load(branch.size(), 0);
+    for (uint32_t i : order) {
+        const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += bp.reqs[i].items;
+        CU_TRY(ctx, launch_project(bp.reqs[i].a, bp.mode, bp.acc, 0, branch[k]));
+    }
+    for (size_t k = 0; k < branch.size(); ++k) {
+        CU_TRY(ctx, cudaEventRecord(ev[k + 1], branch[k]));
+        CU_TRY(ctx, cudaStreamWaitEvent(st, ev[k + 1], 0));
+    }
+    return CTLCU_OK;
+}
+
+// Captures the plan's batch in `form` into an instantiated graph.
+int capture_plan(ctlcu_plan* p, int form, cudaGraph_t* graph, cudaGraphExec_t* exec)
+{
+    ctlcu_ctx* ctx = p->ctx;
+    *graph = nullptr;
+    *exec = nullptr;
+    const size_t n_branch = std::min<size_t>(4, p->bp.reqs.size());
+    cudaStream_t cs = nullptr;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> ev;
+    int r = CTLCU_OK;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+        r = fail(ctx, CTLCU_ERR_CUDA, "stream creation failed");
+    for (size_t k = 0; r == CTLCU_OK && form == CTLCU_PLAN_GRIDS && k < n_branch; ++k) {
+        cudaStream_t b = nullptr;
+        if (cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking) != cudaSuccess)
+            r = fail(ctx, CTLCU_ERR_CUDA, "stream creation failed");
+        else
+            branch.push_back(b);
+    }
+    for (size_t k = 0; r == CTLCU_OK && form == CTLCU_PLAN_GRIDS && k <= n_branch; ++k) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            r = fail(ctx, CTLCU_ERR_CUDA, "event creation failed");
+        else
+            ev.push_back(e);
+    }
+    if (r == CTLCU_OK) {
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed to start");
+        } else {
+            const uint64_t before = ctx->launches;
+            r = form == CTLCU_PLAN_GRIDS ? enqueue_batch_grids(ctx, p->bp, p->bd, cs, branch, ev)
+                                         : enqueue_batch(ctx, p->bp, p->bd, &p->settings, cs);
+            ctx->launches = before;  // counted per replay instead
+            const cudaError_t e = cudaStreamEndCapture(cs, graph);
+            if (r == CTLCU_OK && e != cudaSuccess)
+                r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+            if (r == CTLCU_OK && cudaGraphInstantiate(exec, *graph, 0) != cudaSuccess)
+                r = fail(ctx, CTLCU_ERR_CUDA, "graph instantiation failed");
+        }
+    }
+    for (cudaEvent_t e : ev)
+        cudaEventDestroy(e);
+    for (cudaStream_t b : branch)
+        cudaStreamDestroy(b);
+    if (cs)
+        cudaStreamDestroy(cs);
+    if (r) {
+        if (*exec)
+            cudaGraphExecDestroy(*exec);
+        if (*graph)
+            cudaGraphDestroy(*graph);
+        *graph = nullptr;
+        *exec = nullptr;
+    }
+    return r;
+}
+
+// Mean replay time (ms) of `exec` on the context's stream: one untimed replay, then 3.
+int time_plan(ctlcu_ctx* ctx, cudaGraphExec_t exec, float* ms)
+{
+    cudaEvent_t a = nullptr, b = nullptr;
+    CU_TRY(ctx, cudaEventCreate(&a));
+    cudaError_t e = cudaEventCreate(&b);
+    if (e == cudaSuccess)
+        e = cudaGraphLaunch(exec, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(a, ctx->stream);
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+        e = cudaGraphLaunch(exec, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaEventSynchronize(b);
+    if (e == cudaSuccess)
+        e = cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    if (b)
+        cudaEventDestroy(b);
+    if (e != cudaSuccess)
+        return fail(ctx, CTLCU_ERR_CUDA, "timing the plan failed: %s", cudaGetErrorString(e));
+    *ms /= 3.0f;
+    return CTLCU_OK;
+}
+
+}  // namespace
 
 int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
                       const ctlcu_settings* settings, ctlcu_plan** out)
@@ -1471,29 +1593,38 @@ int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_
                  "plans need the cell kernel (software trilinear, volumeUpSampling 1)");
     if (r == CTLCU_OK)
         r = upload_batch(ctx, p->bp, ctx->stream, false, p->bd);
-    cudaStream_t cs = nullptr;
-    if (r == CTLCU_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
-        r = fail(ctx, CTLCU_ERR_CUDA, "stream creation failed");
     if (r == CTLCU_OK) {
         // descriptors must be on the device before the graph is first replayed
         cudaStreamSynchronize(ctx->stream);
-        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed to start");
-        else {
-            const uint64_t before = ctx->launches;
-            r = enqueue_batch(ctx, p->bp, p->bd, settings, cs);
-            ctx->launches = before;  // counted per replay instead
-            cudaGraph_t g = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(cs, &g);
-            if (r == CTLCU_OK && e != cudaSuccess)
-                r = fail(ctx, CTLCU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-            p->graph = g;
-            if (r == CTLCU_OK && cudaGraphInstantiate(&p->exec, g, 0) != cudaSuccess)
-                r = fail(ctx, CTLCU_ERR_CUDA, "graph instantiation failed");
+        // both forms are captured and timed once; the faster one is kept
+        cudaGraph_t g[2] = { nullptr, nullptr };
+        cudaGraphExec_t x[2] = { nullptr, nullptr };
+        for (int f = 0; f < 2 && r == CTLCU_OK; ++f)
+            r = capture_plan(p, f, &g[f], &x[f]);
+        for (int f = 0; f < 2 && r == CTLCU_OK; ++f)
+            r = time_plan(ctx, x[f], &p->ms[f]);
+        if (r == CTLCU_OK) {
+            // a singular matrix raised while timing is reported again by the replays' ctlcu_sync
+            r = read_flags(ctx);
+            if (r == CTLCU_ERR_SINGULAR_GEOMETRY)
+                r = CTLCU_OK;
         }
+        const int keep = (r == CTLCU_OK && p->ms[CTLCU_PLAN_GRIDS] < p->ms[CTLCU_PLAN_PERSISTENT])
+                             ? CTLCU_PLAN_GRIDS : CTLCU_PLAN_PERSISTENT;
+        for (int f = 0; f < 2; ++f) {
+            if (f == keep && r == CTLCU_OK) {
+                p->graph = g[f];
+                p->exec = x[f];
+            } else {
+                if (x[f])
+                    cudaGraphExecDestroy(x[f]);
+                if (g[f])
+                    cudaGraphDestroy(g[f]);
+            }
+        }
+        p->form = keep;
+        p->launches_per_replay = keep == CTLCU_PLAN_GRIDS ? 1 + (uint64_t)n_requests : 2;
     }
-    if (cs)
-        cudaStreamDestroy(cs);
     if (r) {
         if (p->exec)
             cudaGraphExecDestroy(p->exec);
@@ -1511,6 +1642,19 @@ int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_
     return CTLCU_OK;
 }
 
+int ctlcu_plan_info(const ctlcu_plan* plan, int* form, float* ms_persistent, float* ms_grids)
+{
+    if (!plan)
+        return CTLCU_ERR_INVALID_ARGUMENT;
+    if (form)
+        *form = plan->form;
+    if (ms_persistent)
+        *ms_persistent = plan->ms[CTLCU_PLAN_PERSISTENT];
+    if (ms_grids)
+        *ms_grids = plan->ms[CTLCU_PLAN_GRIDS];
+    return CTLCU_OK;
+}
+
 int ctlcu_plan_launch(ctlcu_plan* plan, void* stream)
 {
     TraceRange trace_("ctlcu_plan_launch");
@@ -1521,7 +1665,7 @@ int ctlcu_plan_launch(ctlcu_plan* plan, void* stream)
     cudaSetDevice(ctx->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     CU_TRY(ctx, cudaGraphLaunch(plan->exec, st));
-    ctx->launches += 2;
+    ctx->launches += plan->launches_per_replay;
     return CTLCU_OK;
 }
 

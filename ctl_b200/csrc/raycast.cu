@@ -324,6 +324,8 @@ __device__ __forceinline__ uint32_t cell_index(float2 kk, const CellFrame& fr, f
 }
 #endif
 
+#if !CTLCU_CELL_PAIRED
+// (the one-sample loop; the paired loop below uses cell_sample_pair)
 __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const char* __restrict__ cells, float2 kk,
                                              const CellFrame& fr, float2 dxy, float dz, uint32_t sy, uint32_t sz,
                                              uint32_t cmax, CellCache& cc)
@@ -385,6 +387,8 @@ __device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const cha
     const float2 g = __ffma2_rn(make_float2(hxy.y, hxy.y), eb, ea);
     return fmaf(hz, g.y, g.x);
 }
+
+#endif
 
 #if CTLCU_CELL_PAIRED
 // The interpolant of the cached cell at offsets (hx, hy, hz) from its centre,
@@ -649,32 +653,73 @@ __device__ __forceinline__ bool pixel_of(const ProjectArgs& a, uint32_t& vm, uin
     return pixel_of_thread(a, threadIdx.x, vm, x, y);
 }
 
+// Writes the warp's pixel values (called by all 32 lanes): each lane holds
+// `val` for pixel (vm, x, y), or ok = false for no pixel.  Four consecutive
+// lanes are four consecutive channels of one detector row (a warp patch is 4
+// or 8 channels wide), so where all four pixels exist and their row segment
+// starts on a 16-byte boundary, the quad's first lane gathers the other three
+// values and writes the segment as one 16-byte store; otherwise each lane
+// stores its own value.
+__device__ __forceinline__ void store_patch(const ProjectArgs& a, uint32_t vm, uint32_t x, uint32_t y, float val,
+                                            bool ok)
+{
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u, lead = lane & ~3u;
+    const float v1 = __shfl_down_sync(full, val, 1);
+    const float v2 = __shfl_down_sync(full, val, 2);
+    const float v3 = __shfl_down_sync(full, val, 3);
+    const uint32_t okmask = __ballot_sync(full, ok);
+    float* dst = a.out + ((size_t)vm * a.rows + y) * a.channels + x;
+    const bool whole = ((okmask >> lead) & 0xfu) == 0xfu && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0;
+    // the quad's choice is its first lane's
+    const bool vec = __shfl_sync(full, whole ? 1 : 0, lead) != 0;
+    if (vec) {
+        if (lane == lead)
+            *reinterpret_cast<float4*>(dst) = make_float4(val, v1, v2, v3);
+    } else if (ok) {
+        *dst = val;
+    }
+}
+
 // The rays of work item `b` for thread `tid`, cell or pair loop (FP32 entries).
+// Called by every lane of a warp (the store is warp-cooperative).
 template <Mode M, Accum ACC, int U>
 __device__ __forceinline__ void cells_item(const ProjectArgs& a, uint32_t b, uint32_t tid)
 {
     uint32_t vm, x, y;
-    if (!pixel_of_item(a, b, tid, vm, x, y))
-        return;
-    const ViewGeom& g = a.geom[vm];
-    float* dst = a.out + ((size_t)vm * a.rows + y) * a.channels + x;
-    if (!g.valid) {
-        *dst = 0.0f;
-        return;
-    }
-    Accumulator<ACC> acc;
-    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
-    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
-        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
-            const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
-            const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
-            const Ray r = setup_ray<M>(a, g, px, py, a.flags);
-            if (M == Mode::Pairs)
-                march_pairs<ACC, U>(a, r, acc);
-            else
-                march_cells<ACC, U>(a, r, acc);
+    const bool ok = pixel_of_item(a, b, tid, vm, x, y);
+    float val = 0.0f;
+    if (ok) {
+        const ViewGeom& g = a.geom[vm];
+        if (g.valid) {
+            Accumulator<ACC> acc;
+            if (a.rays_x == 1 && a.rays_y == 1) {
+                // one ray through the pixel centre (x - 0.5 + 0.5 is x exactly): the
+                // pixel and its geometry are dead once the ray is set up, so the
+                // sample loop carries only the ray
+                const Ray r = setup_ray<M>(a, g, (double)x, (double)y, a.flags);
+                if (M == Mode::Pairs)
+                    march_pairs<ACC, U>(a, r, acc);
+                else
+                    march_cells<ACC, U>(a, r, acc);
+            } else {
+                const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+                for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+                    for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+                        const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
+                        const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
+                        const Ray r = setup_ray<M>(a, g, px, py, a.flags);
+                        if (M == Mode::Pairs)
+                            march_pairs<ACC, U>(a, r, acc);
+                        else
+                            march_cells<ACC, U>(a, r, acc);
+                    }
+            }
+            val = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
         }
-    *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
+    }
+    // the pixel again for the store, rather than holding it through the loop
+    pixel_of_item(a, b, tid, vm, x, y);
+    store_patch(a, vm, x, y, val, ok);
 }
 
 // Cell or pair loop over one block of the regular grid.
@@ -736,29 +781,29 @@ __global__ void __maxnreg__(CTLCU_GATHER_MAXREG) project_kernel(const ProjectArg
 {
     static_assert(M == Mode::Trilinear || M == Mode::Nearest || M == Mode::Texture, "cells_kernel runs these");
     uint32_t vm, x, y;
-    if (!pixel_of(a, vm, x, y))
-        return;
-    const ViewGeom& g = a.geom[vm];
-    float* dst = a.out + ((size_t)vm * a.rows + y) * a.channels + x;
-    if (!g.valid) {
-        *dst = 0.0f;
-        return;
-    }
-    Accumulator<ACC> acc;
-    const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
-    for (uint32_t rx = 0; rx < a.rays_x; ++rx)
-        for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
-            const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
-            const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
-            const Ray r = setup_ray<M>(a, g, px, py, a.flags);
-            if (M == Mode::Trilinear)
-                march_trilinear<T, ACC, UP>(a, r, acc);
-            else if (M == Mode::Nearest)
-                march_nearest<T, ACC>(a, r, acc);
-            else
-                march_texture<ACC>(a, r, acc);
+    const bool ok = pixel_of(a, vm, x, y);
+    float val = 0.0f;
+    if (ok) {
+        const ViewGeom& g = a.geom[vm];
+        if (g.valid) {
+            Accumulator<ACC> acc;
+            const double ix = 1.0 / a.rays_x, iy = 1.0 / a.rays_y;
+            for (uint32_t rx = 0; rx < a.rays_x; ++rx)
+                for (uint32_t ry = 0; ry < a.rays_y; ++ry) {
+                    const double px = (double)x - 0.5 + 0.5 * ix + rx * ix;
+                    const double py = (double)y - 0.5 + 0.5 * iy + ry * iy;
+                    const Ray r = setup_ray<M>(a, g, px, py, a.flags);
+                    if (M == Mode::Trilinear)
+                        march_trilinear<T, ACC, UP>(a, r, acc);
+                    else if (M == Mode::Nearest)
+                        march_nearest<T, ACC>(a, r, acc);
+                    else
+                        march_texture<ACC>(a, r, acc);
+                }
+            val = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
         }
-    *dst = static_cast<float>(a.increment * acc.value() / (double)(a.rays_x * a.rays_y));
+    }
+    store_patch(a, vm, x, y, val, ok);
 }
 
 template <Mode M>

@@ -282,6 +282,13 @@ class Plan:
     def launch(self, stream: int = 0) -> None:
         self.ctx._check(self.ctx.lib.ctlcu_plan_launch(self.h, C.c_void_p(stream or None)))
 
+    def info(self) -> dict:
+        """ctlcu_plan_info: the form the plan kept and both forms' replay times (ms)."""
+        form, a, b = C.c_int(0), C.c_float(0), C.c_float(0)
+        self.ctx._check(self.ctx.lib.ctlcu_plan_info(self.h, C.byref(form), C.byref(a), C.byref(b)))
+        return {"form": "grids" if form.value == L.PLAN_GRIDS else "persistent",
+                "ms_persistent": float(a.value), "ms_grids": float(b.value)}
+
     def close(self) -> None:
         if self.h:
             self.ctx._check(self.ctx.lib.ctlcu_plan_destroy(self.h))

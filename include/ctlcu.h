@@ -208,8 +208,8 @@ CTLCU_API int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests,
 
 /*
  * Plans: a batch prepared once (descriptors on the device, cell arrays built)
- * and captured as a CUDA graph of its setup and persistent projection
- * launches; each ctlcu_plan_launch replays it on `stream`.  The requests'
+ * and captured as a CUDA graph of its setup and projection launches (in the
+ * faster of two forms, below); each ctlcu_plan_launch replays it on `stream`.  The requests'
  * pmats/out pointers are fixed in the plan -- update their contents in place
  * between launches.  Plans need the cell kernel; their volumes cannot be
  * released (CTLCU_ERR_BUSY) until the plan is destroyed.
@@ -219,6 +219,19 @@ CTLCU_API int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, u
                                 const ctlcu_settings* settings, ctlcu_plan** plan);
 CTLCU_API int ctlcu_plan_launch(ctlcu_plan* plan, void* stream);
 CTLCU_API int ctlcu_plan_destroy(ctlcu_plan* plan);
+
+/* The two forms a plan's graph can hold.  ctlcu_plan_create captures both,
+ * replays each once untimed and three times timed (writing the outputs), and
+ * keeps the faster:
+ *   PERSISTENT  the setup and one persistent launch over every request's work
+ *               items (warp patches taken from one queue);
+ *   GRIDS       the setup and one grid launch per request, the requests dealt
+ *               out longest first over up to 4 parallel graph branches, so that
+ *               launches overlap and fill each other's last waves.
+ * Both forms give the same bits. */
+typedef enum { CTLCU_PLAN_PERSISTENT = 0, CTLCU_PLAN_GRIDS = 1 } ctlcu_plan_form;
+/* The form a plan kept and the replay times (ms) measured for both at its creation. */
+CTLCU_API int ctlcu_plan_info(const ctlcu_plan* plan, int* form, float* ms_persistent, float* ms_grids);
 
 /* ---- several devices ---------------------------------------------------------------------- */
 
