@@ -988,6 +988,42 @@ int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, co
     return CTLCU_OK;
 }
 
+// The batch as one grid launch per request (the single-request kernel, whose
+// arguments sit in the constant bank), dealt out longest first over `branch`
+// streams that fork from and join back into `st`: launches of different
+// requests overlap, so one fills the SMs that another's last wave leaves idle.
+// With no branches, the launches go in order on `st`.
+int enqueue_batch_grids(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, cudaStream_t st,
+                        const std::vector<cudaStream_t>& branch, const std::vector<cudaEvent_t>& ev)
+{
+    const uint32_t n = (uint32_t)bp.reqs.size();
+    CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
+    if (branch.empty()) {
+        for (uint32_t i = 0; i < n; ++i)
+            CU_TRY(ctx, launch_project(bp.reqs[i].a, bp.mode, bp.acc, 0, st));
+        return CTLCU_OK;
+    }
+    CU_TRY(ctx, cudaEventRecord(ev[0], st));
+    for (cudaStream_t b : branch)
+        CU_TRY(ctx, cudaStreamWaitEvent(b, ev[0], 0));
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i)
+        order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return bp.reqs[x].items > bp.reqs[y].items; });
+    std::vector<uint64_t> load(branch.size(), 0);
+    for (uint32_t i : order) {
+        const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += bp.reqs[i].items;
+        CU_TRY(ctx, launch_project(bp.reqs[i].a, bp.mode, bp.acc, 0, branch[k]));
+    }
+    for (size_t k = 0; k < branch.size(); ++k) {
+        CU_TRY(ctx, cudaEventRecord(ev[k + 1], branch[k]));
+        CU_TRY(ctx, cudaStreamWaitEvent(st, ev[k + 1], 0));
+    }
+    return CTLCU_OK;
+}
+
 void free_batch(BatchDevice& bd, cudaStream_t st, bool pooled)
 {
     void* ptrs[4] = { bd.geom, bd.setups, bd.reqs, bd.counter };
@@ -1426,10 +1462,17 @@ int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t 
         }
         return CTLCU_OK;
     }
+    // one grid launch per request, in order on `st`: the single-request kernel
+    // keeps its arguments in the constant bank, where the persistent kernel of
+    // plans reads them from shared memory, and measured no slower on every batch
+    // tried.  Batches on other streams (the DRR server runs two) fill the SMs
+    // that one request's last wave leaves idle.
     BatchDevice bd;
     r = upload_batch(ctx, bp, st, true, bd);
     if (r == CTLCU_OK)
-        r = enqueue_batch(ctx, bp, bd, settings, st);
+        r = enqueue_batch_grids(ctx, bp, bd, st, {}, {});
+    if (r == CTLCU_OK)
+        ctx->launches += 1 + (uint64_t)n_requests;
     free_batch(bd, st, true);
     return r;
 }
@@ -1450,36 +1493,6 @@ struct ctlcu_plan {
 };
 
 namespace {
-
-// The batch as one grid launch per request (the single-request kernel, whose
-// arguments sit in the constant bank), dealt out longest first over `branch`
-// streams that fork from and join back into `st`: launches of different
-// requests overlap, so one fills the SMs that another's last wave leaves idle.
-int enqueue_batch_grids(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, cudaStream_t st,
-                        const std::vector<cudaStream_t>& branch, const std::vector<cudaEvent_t>& ev)
-{
-    const uint32_t n = (uint32_t)bp.reqs.size();
-    CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
-    CU_TRY(ctx, cudaEventRecord(ev[0], st));
-    for (cudaStream_t b : branch)
-        CU_TRY(ctx, cudaStreamWaitEvent(b, ev[0], 0));
-    std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; ++i)
-        order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t x, uint32_t y) { return bp.reqs[x].items > bp.reqs[y].items; });
-    std::vector<uint64_t> load(branch.size(), 0);
-    for (uint32_t i : order) {
-        const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
-        load[k] += bp.reqs[i].items;
-        CU_TRY(ctx, launch_project(bp.reqs[i].a, bp.mode, bp.acc, 0, branch[k]));
-    }
-    for (size_t k = 0; k < branch.size(); ++k) {
-        CU_TRY(ctx, cudaEventRecord(ev[k + 1], branch[k]));
-        CU_TRY(ctx, cudaStreamWaitEvent(st, ev[k + 1], 0));
-    }
-    return CTLCU_OK;
-}
 
 // Captures the plan's batch in `form` into an instantiated graph.
 int capture_plan(ctlcu_plan* p, int form, cudaGraph_t* graph, cudaGraphExec_t* exec)

@@ -198,10 +198,12 @@ CTLCU_API int ctlcu_project_volume(ctlcu_ctx* ctx, const ctlcu_volume_desc* desc
                          uint32_t n_modules, uint32_t channels, uint32_t rows, float* out);
 
 /*
- * Batched form: every request's views in one persistent launch (a work list
- * of (request, view, module, tile) items over all SMs).  Requests may use
+ * Batched form: one setup launch for every request's geometry, then each
+ * request's projection launch, in order on `stream`.  Requests may use
  * different volumes and detector sizes.  All pointers are device memory;
- * asynchronous on `stream` (NULL = the context's stream).
+ * asynchronous on `stream` (NULL = the context's stream).  Plans
+ * (ctlcu_plan_create) capture a batch once and can also run it as one
+ * persistent launch.
  */
 CTLCU_API int ctlcu_project_batch(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
                         const ctlcu_settings* settings, void* stream);
