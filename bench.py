@@ -20,8 +20,8 @@ roofline the ray-casting kernel's gather bytes (samples x 8 taps x voxel bytes +
          output) per launch over its CUDA-event duration, against on-SM L1
          delivery (SMs x 128 B/clk x sampled SM clock)
 legs     (one GPU) the rest of the headline metric on the same workload: the
-         batched BF16 form (BF16 storage, 8 requests of 45 views in one
-         persistent launch replayed from a CUDA graph), the plain FP32 gather
+         batched BF16 form (BF16 storage, 8 requests of 45 views, one CUDA
+         graph replay per step: a plan), the plain FP32 gather
          loop it is compared with, the FP64 accumulator, and DRR serving
          latency (8 x 256^3 BF16, Poisson 2000 requests/s)
 --impl reference   the reference's own kernel (raycasterprojector_interp.cl
@@ -59,7 +59,7 @@ WORKLOAD = "256^3 f32 ellipsoid phantom -> 360 x 512^2 short-scan (200 deg + fan
 # workload, from one ncu capture (profiles/cells_kernel_256cubed_to_512sq_dram.md),
 # with the launch shape it was captured at (views per block, lanes_x, rays per block, unroll)
 # and its accumulator
-CELLS_TRAFFIC_BYTES = 7.895376896e9 + 0.763993344e9
+CELLS_TRAFFIC_BYTES = 7.883831808e9 + 0.424111872e9
 CELLS_TRAFFIC_SHAPE = (2, 4, 256, 4)
 CELLS_TRAFFIC_ACCUM = "kahan"
 
@@ -440,7 +440,7 @@ def run_legs(args, ctx, vobj, volume, P, flush, stream, value_fp32):
     legs["plain_gather_fp32"] = {"value": plain, "unit": "projections/s", "ms_per_step": statistics.mean(ms),
                                  "what": "FP32 storage, gather loop (8 scalar loads per sample), Kahan accumulator"}
     # the batched BF16 form: BF16 storage, 8 requests of 45 views (clients of one volume)
-    # in one persistent launch, replayed from a CUDA graph (ctlcu_plan_launch)
+    # in one CUDA graph replay (ctlcu_plan_launch), in the plan's faster form
     vb = ctx.volume(vobj, L.BF16)
     ctx.autotune(vb, P, CHANNELS, ROWS, Settings())
     parts = L.split_views(V, 8)
@@ -449,8 +449,9 @@ def run_legs(args, ctx, vobj, volume, P, flush, stream, value_fp32):
     ms = _time_steps(lambda: plan.launch(ctx.stream), args.steps, args.warmup, stream, flush.zero_)
     batched = rate(ms)
     legs["batched_bf16"] = {"value": batched, "unit": "projections/s", "ms_per_step": statistics.mean(ms),
-                            "what": "BF16 storage, 8 requests x 45 views, one persistent launch per step "
-                                    "replayed from a CUDA graph (ctlcu_plan_launch)",
+                            "what": "BF16 storage, 8 requests x 45 views, one CUDA graph replay per step "
+                                    "(ctlcu_plan_launch)",
+                            "plan": plan.info(),
                             "vs_plain_gather_fp32": batched / plain, "vs_drop_in_fp32": batched / value_fp32}
     plan.close()
     del reqs
@@ -906,7 +907,7 @@ SEED_NOISE = 20240611
 
 
 def run_c4(args):
-    """64 uneven volumes: one persistent launch replayed from a CUDA graph vs 64 sequential calls."""
+    """64 uneven volumes: one plan (a CUDA graph replay) vs 64 sequential calls."""
     import torch
 
     from ctl_b200 import _lib as L
@@ -931,13 +932,14 @@ def run_c4(args):
                 ctx.project(v, P, j.channels, j.rows, s, out=out, stream=ctx.stream)
         ms_seq = _time_device(lambda: sequential(L.KERNEL_CELLS), max(2, args.steps // 3), 1, stream)
         ms_plain = _time_device(lambda: sequential(L.KERNEL_GATHER), max(2, args.steps // 3), 1, stream)
+        info = plan.info()
         plan.close()
         v_plan = total_views / (statistics.mean(ms_plan) / 1e3)
         _line(f"projections/s, 64 uneven volumes batched ({storage_name} storage)", v_plan, "projections/s",
               statistics.mean(ms_plan), args,
               {"workload": "64 volumes (edges 96-256), 30-360 views each, detectors 256^2-768x512",
                "views_per_step": total_views, "storage": storage_name},
-              sequential_cells_views_per_s=total_views / (statistics.mean(ms_seq) / 1e3),
+              plan=info, sequential_cells_views_per_s=total_views / (statistics.mean(ms_seq) / 1e3),
               sequential_plain_gather_views_per_s=total_views / (statistics.mean(ms_plain) / 1e3))
         for v in vols:
             v.release()
@@ -958,7 +960,7 @@ def drr_measurements(ctx, args, sweep: bool = True) -> dict:
     kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
               "pairs": L.KERNEL_PAIRS}[args.kernel]
     settings = Settings(kernel=kernel)
-    # 2 streams and batches of at most 24 views: a batch's persistent launch holds the SMs
+    # 2 streams and batches of at most 24 views: a batch's launches hold the SMs
     # until it is done, so bounding its views bounds how long later requests wait behind it
     server = DRRServer(ctx, vols, 256, 256, settings, streams=2, max_batch=256,
                        budget_bytes=40 * 10**9, max_batch_views=24)

@@ -10,18 +10,19 @@ the device and requests are batched as they arrive:
   unfinished requests (their projection matrices and images) stays within the
   budget; otherwise it waits in the arrival queue (or is refused if `refuse`);
 * batching: whenever one of `streams` CUDA streams is free, every queued
-  request (up to `max_batch`) goes into one persistent launch on it
-  (ctlcu_project_batch), so requests that arrive while others run are picked
-  up as soon as a stream frees and their work overlaps on the device; the
+  request (up to `max_batch`) goes into one batch on it (ctlcu_project_batch:
+  one setup launch, then the requests' projection launches), so requests that
+  arrive while others run are picked up as soon as a stream frees and their
+  work overlaps on the device; the
   batch's matrices go through the stream's pinned staging buffer with a
   non-blocking copy, and its outputs are one allocation sliced per request;
 * timing: latency is arrival (host clock) to the end of the request's batch
   on the device (CUDA event), with the device clock tied to the host clock
   at start.
 
-The projections of a request depend only on its own inputs: the persistent
-kernel computes every work item independently, so a result is the same alone
-and in any mix (tests/test_gpu_serving.py checks this).
+The projections of a request depend only on its own inputs: every ray is
+computed independently of the others in its batch, so a result is the same
+alone and in any mix (tests/test_gpu_serving.py checks this).
 """
 from __future__ import annotations
 
@@ -86,7 +87,7 @@ class DRRServer:
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.max_batch = max_batch
         # a batch stops taking requests once it holds this many views (the first request
-        # always goes in).  A batch's persistent launch holds the SMs until it is done, so
+        # always goes in).  A batch's launches hold the SMs until they are done, so
         # batches on other streams wait behind it; bounding its views bounds that wait.
         self.max_batch_views = max_batch_views
         self.refuse = refuse
