@@ -35,6 +35,12 @@ import numpy as np
 from .projector import Context, Settings, Volume, torch_stream_handle
 
 
+# torch's caching allocator serves requests of up to 1 MiB from a separate
+# pool of small blocks; one float more than that puts a batch's outputs in the
+# large-block pool that DRRServer.reserve() fills
+_LARGE_FLOATS = (1 << 20) // 4 + 1
+
+
 @dataclass
 class DRRRequest:
     rid: int
@@ -77,7 +83,7 @@ class DRRServer:
     def __init__(self, ctx: Context, volumes: Sequence[Volume], channels: int, rows: int,
                  settings: Optional[Settings] = None, streams: int = 2, max_batch: int = 256,
                  budget_bytes: int = 40 * 10**9, refuse: bool = False, deadline_ms: Optional[float] = None,
-                 max_batch_views: Optional[int] = None):
+                 max_batch_views: Optional[int] = None, reserve_bytes: int = 0):
         import torch
         self.torch = torch
         self.ctx = ctx
@@ -103,6 +109,25 @@ class DRRServer:
         # overwrites matrices that are still being copied or read.
         self._pin = [None] * streams
         self._dev = [None] * streams
+        if reserve_bytes > 0:
+            self.reserve(min(int(reserve_bytes), self._free_budget()))
+
+    def reserve(self, nbytes: int) -> None:
+        """Allocate nbytes of device memory for results up front, split over the
+        server's streams, and hand it back to torch's caching allocator, which keeps
+        it for later allocations on the same stream.  A batch's output allocation is
+        then carved from it instead of growing the allocator while requests wait:
+        growing it took 20-28 ms per new segment, during which no batch was launched.
+        The memory stays reserved for this process (torch.cuda.empty_cache() returns
+        whatever is unused)."""
+        torch = self.torch
+        per = int(nbytes) // len(self.streams)
+        if per <= 0:
+            return
+        for s in self.streams:
+            with torch.cuda.stream(s):
+                block = torch.empty(per, dtype=torch.uint8, device="cuda")
+            del block
 
     def _free_budget(self) -> int:
         """Budget left for requests after the resident volumes (with their cell arrays)."""
@@ -132,19 +157,27 @@ class DRRServer:
             dP = torch.from_numpy(P).cuda()
             keep.append((dP, out))
             self.ctx.project_batch([(v, dP, out)], self.settings, stream=stream)
+        # the staging buffers of every stream, before the first request
+        for i in range(len(self.streams)):
+            self._ensure_stage(i, 1)
         torch.cuda.synchronize()
         self.ctx.sync()
+
+    def _ensure_stage(self, i: int, n: int) -> None:
+        """Stream i's staging buffers hold at least n view-modules' matrices."""
+        torch = self.torch
+        if self._pin[i] is None or self._pin[i].shape[0] < n:
+            cap = max(n, 256)
+            with torch.cuda.stream(self.streams[i]):
+                self._pin[i] = torch.empty((cap, 12), dtype=torch.float64).pin_memory()
+                self._dev[i] = torch.empty((cap, 12), dtype=torch.float64, device="cuda")
 
     def _stage(self, i: int, batch: Sequence[DRRRequest]):
         """The batch's matrices gathered into stream i's pinned staging buffer and
         copied to its device buffer without blocking the host (on the current
         stream, which is stream i): an (n_view_modules, 12) float64 device view."""
-        torch = self.torch
         n = sum(int(r.pmats.shape[0] * r.pmats.shape[1]) for r in batch)
-        if self._pin[i] is None or self._pin[i].shape[0] < n:
-            cap = max(n, 256)
-            self._pin[i] = torch.empty((cap, 12), dtype=torch.float64).pin_memory()
-            self._dev[i] = torch.empty((cap, 12), dtype=torch.float64, device="cuda")
+        self._ensure_stage(i, n)
         host = self._pin[i].numpy()
         at = 0
         for r in batch:
@@ -234,9 +267,13 @@ class DRRServer:
                     batch, queue = queue[:take], queue[take:]
                     with torch.cuda.stream(s):
                         allP = self._stage(i, batch)
-                        # one output allocation per batch; each request keeps its slice
+                        # one output allocation per batch; each request keeps its slice.  It
+                        # is at least _LARGE_FLOATS long, so that it comes from the caching
+                        # allocator's large-block pool, which reserve() fills up front
                         n_vm = allP.shape[0]
-                        outs = torch.empty((n_vm, self.rows, self.channels), device="cuda")
+                        per = self.rows * self.channels
+                        flat = torch.empty(max(n_vm * per, _LARGE_FLOATS), device="cuda")
+                        outs = flat[: n_vm * per].view(n_vm, self.rows, self.channels)
                         items, at = [], 0
                         for r in batch:
                             V, M = r.pmats.shape[:2]

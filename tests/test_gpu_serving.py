@@ -102,3 +102,30 @@ def test_server_deadline_refuses_late_requests():
     assert all(r.done >= r.arrival for r in served)
     h.release()
     ctx.close()
+
+
+def test_reserved_server_allocates_nothing_while_serving():
+    """With reserve_bytes, the server's result memory is allocated before serving: a run
+    grows no device segment (each growth of the caching allocator held up the request
+    loop by tens of ms), and its results are the single-call results."""
+    import torch
+
+    from ctl_b200 import _lib as L
+    ctx = Context(0)
+    vol = Ph.ellipsoid_phantom((32, 32, 32), (3, 3, 3), 4, seed=13)
+    h = ctx.volume(VoxelVolume(vol, (3, 3, 3)), L.BF16)
+    server = DRRServer(ctx, [h], 48, 40, Settings(), streams=2, max_batch=8, reserve_bytes=256 << 20)
+    server.warm_up()
+    reqs = poisson_requests(20000.0, 50, 1, _base_view(), seed=17, views=(1, 4))
+    torch.cuda.synchronize()
+    before = torch.cuda.memory_stats().get("segment.all.allocated", 0)
+    stats = server.run(reqs)
+    after = torch.cuda.memory_stats().get("segment.all.allocated", 0)
+    assert stats.completed == 50
+    assert after == before, (before, after)
+    for r in reqs[::7]:
+        alone = ctx.project(h, r.pmats, 48, 40, Settings())
+        np.testing.assert_array_equal(r.out.cpu().numpy(), alone)
+    del reqs
+    h.release()
+    ctx.close()
