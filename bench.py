@@ -915,7 +915,7 @@ def run_c4(args):
     from ctl_b200.projector import Context, Settings, VoxelVolume
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    jobs = W.c4()
+    jobs = W.c4(n_volumes=args.volumes)
     total_views = sum(j.pmats.shape[0] for j in jobs)
     for storage_name, storage in (("f32", L.F32), ("bf16", L.BF16)):
         vols = [ctx.volume(VoxelVolume(j.volume, j.voxel), storage) for j in jobs]
@@ -1050,6 +1050,8 @@ def main():
                     default="c2",
                     help="c2 (default) is the headline; the others print extra lines")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--volumes", type=int, default=64,
+                    help="c4: the first N of the 64 uneven volumes (fewer = a small profiling case)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the one-GPU legs (FP64 accumulator, gather, batched BF16, DRR serving)")
     args = ap.parse_args()
