@@ -989,7 +989,7 @@ def drr_measurements(ctx, args, sweep: bool = True) -> dict:
     n_views = sum(int(r.pmats.shape[0]) for r in stream_2000)
     span_s = n_req / rate
     # offered-rate sweep: the highest rate whose p99 stays under 5 ms
-    fracs = (0.2, 0.35, 0.5, 0.65, 0.8) if sweep else (0.35, 0.5, 0.65)
+    fracs = (0.2, 0.35, 0.5, 0.65, 0.75, 0.85) if sweep else (0.35, 0.5, 0.65, 0.75)
     points = []
     for frac in fracs:
         r_off = frac * cap["throughput_req_s"]
