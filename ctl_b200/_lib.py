@@ -31,7 +31,7 @@ KERNEL_AUTO, KERNEL_GATHER, KERNEL_CELLS, KERNEL_PAIRS = 0, 1, 2, 3
 # the default stream (torch's default) must name it with this handle.
 STREAM_LEGACY = 1
 NOALLOC_MAX_VIEW_MODULES = 4096
-PLAN_PERSISTENT, PLAN_GRIDS = 0, 1  # ctlcu_plan_form  # scratch entries of ctlcu_project_noalloc
+PLAN_CHOOSE, PLAN_PERSISTENT, PLAN_GRIDS = -1, 0, 1  # ctlcu_plan_form  # scratch entries of ctlcu_project_noalloc
 
 STATUS_NAMES = {
     OK: "OK", ERR_INVALID_ARGUMENT: "INVALID_ARGUMENT", ERR_INVALID_HANDLE: "INVALID_HANDLE",
@@ -118,6 +118,8 @@ SIGNATURES = [
     ("ctlcu_plan_launch", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ctlcu_plan_destroy", C.c_int, [C.c_void_p]),
     ("ctlcu_plan_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("ctlcu_plan_create_form", C.c_int, [C.c_void_p, C.POINTER(Request), C.c_uint32, C.POINTER(Settings), C.c_int,
+                                         C.POINTER(C.c_void_p)]),
     ("ctlcu_sync", C.c_int, [C.c_void_p]),
     ("ctlcu_count_samples", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Settings), C.c_void_p, C.c_uint32,
                                       C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),

@@ -968,7 +968,7 @@ int upload_batch(ctlcu_ctx* ctx, BatchPrep& bp, cudaStream_t st, bool pooled, Ba
     CU_TRY(ctx, alloc((void**)&bd.geom, sizeof(ViewGeom) * (size_t)bp.total_vm));
     CU_TRY(ctx, alloc((void**)&bd.setups, sizeof(BatchSetup) * n));
     CU_TRY(ctx, alloc((void**)&bd.reqs, sizeof(BatchReq) * n));
-    CU_TRY(ctx, alloc((void**)&bd.counter, sizeof(unsigned int)));
+    CU_TRY(ctx, alloc((void**)&bd.counter, sizeof(unsigned int) * kBatchCounters));
     for (size_t i = 0; i < n; ++i)
         bp.reqs[i].a.geom = bd.geom + bp.first_vm[i];
     CU_TRY(ctx, cudaMemcpyAsync(bd.setups, bp.setups.data(), sizeof(BatchSetup) * n, cudaMemcpyHostToDevice, st));
@@ -980,7 +980,7 @@ int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, co
                   cudaStream_t st)
 {
     const uint32_t n = (uint32_t)bp.reqs.size();
-    CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int), st));
+    CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int) * kBatchCounters, st));
     CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
     int blocks = 0;
     CU_TRY(ctx, launch_batch(bd.reqs, n, bp.total_items, bp.mode, bp.acc, bp.shape, bd.counter, &blocks, st));
@@ -1585,8 +1585,16 @@ int time_plan(ctlcu_ctx* ctx, cudaGraphExec_t exec, float* ms)
 int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
                       const ctlcu_settings* settings, ctlcu_plan** out)
 {
+    return ctlcu_plan_create_form(ctx, requests, n_requests, settings, CTLCU_PLAN_CHOOSE, out);
+}
+
+int ctlcu_plan_create_form(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                           const ctlcu_settings* settings, int form, ctlcu_plan** out)
+{
     if (!ctx || !out)
         return CTLCU_ERR_INVALID_ARGUMENT;
+    if (form != CTLCU_PLAN_CHOOSE && form != CTLCU_PLAN_PERSISTENT && form != CTLCU_PLAN_GRIDS)
+        return fail(ctx, CTLCU_ERR_INVALID_ARGUMENT, "unknown plan form %d", form);
     std::lock_guard<std::mutex> lk(ctx->mu);
     *out = nullptr;
     if (!requests || n_requests == 0)
@@ -1609,20 +1617,24 @@ int ctlcu_plan_create(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_
     if (r == CTLCU_OK) {
         // descriptors must be on the device before the graph is first replayed
         cudaStreamSynchronize(ctx->stream);
-        // both forms are captured and timed once; the faster one is kept
+        // the requested form, or both forms captured and timed once and the faster kept
         cudaGraph_t g[2] = { nullptr, nullptr };
         cudaGraphExec_t x[2] = { nullptr, nullptr };
         for (int f = 0; f < 2 && r == CTLCU_OK; ++f)
-            r = capture_plan(p, f, &g[f], &x[f]);
-        for (int f = 0; f < 2 && r == CTLCU_OK; ++f)
-            r = time_plan(ctx, x[f], &p->ms[f]);
-        if (r == CTLCU_OK) {
-            // a singular matrix raised while timing is reported again by the replays' ctlcu_sync
-            r = read_flags(ctx);
-            if (r == CTLCU_ERR_SINGULAR_GEOMETRY)
-                r = CTLCU_OK;
+            if (form == CTLCU_PLAN_CHOOSE || form == f)
+                r = capture_plan(p, f, &g[f], &x[f]);
+        if (form == CTLCU_PLAN_CHOOSE) {
+            for (int f = 0; f < 2 && r == CTLCU_OK; ++f)
+                r = time_plan(ctx, x[f], &p->ms[f]);
+            if (r == CTLCU_OK) {
+                // a singular matrix raised while timing is reported again by the replays' ctlcu_sync
+                r = read_flags(ctx);
+                if (r == CTLCU_ERR_SINGULAR_GEOMETRY)
+                    r = CTLCU_OK;
+            }
         }
-        const int keep = (r == CTLCU_OK && p->ms[CTLCU_PLAN_GRIDS] < p->ms[CTLCU_PLAN_PERSISTENT])
+        const int keep = form != CTLCU_PLAN_CHOOSE ? form
+                         : (r == CTLCU_OK && p->ms[CTLCU_PLAN_GRIDS] < p->ms[CTLCU_PLAN_PERSISTENT])
                              ? CTLCU_PLAN_GRIDS : CTLCU_PLAN_PERSISTENT;
         for (int f = 0; f < 2; ++f) {
             if (f == keep && r == CTLCU_OK) {

@@ -556,13 +556,17 @@ class Context:
         self._check(self.lib.ctlcu_project_batch(self.h, arr, len(requests), C.byref(st),
                                                  C.c_void_p(stream or None)))
 
-    def plan(self, requests: Sequence[tuple], settings: Optional[Settings] = None) -> "Plan":
-        """A batch captured once as a CUDA graph; Plan.launch() replays it."""
+    def plan(self, requests: Sequence[tuple], settings: Optional[Settings] = None,
+             form: int = L.PLAN_CHOOSE) -> "Plan":
+        """A batch captured once as a CUDA graph; Plan.launch() replays it.  form:
+        L.PLAN_CHOOSE (time both forms at creation and keep the faster),
+        L.PLAN_PERSISTENT or L.PLAN_GRIDS."""
         settings = settings or Settings()
         arr = self._requests(requests)
         st = settings.to_c()
         h = C.c_void_p()
-        self._check(self.lib.ctlcu_plan_create(self.h, arr, len(requests), C.byref(st), C.byref(h)))
+        self._check(self.lib.ctlcu_plan_create_form(self.h, arr, len(requests), C.byref(st), int(form),
+                                                    C.byref(h)))
         return Plan(self, h, requests)
 
     def sync(self) -> None:

@@ -231,9 +231,14 @@ CTLCU_API int ctlcu_plan_destroy(ctlcu_plan* plan);
  *               out longest first over up to 4 parallel graph branches, so that
  *               launches overlap and fill each other's last waves.
  * Both forms give the same bits. */
-typedef enum { CTLCU_PLAN_PERSISTENT = 0, CTLCU_PLAN_GRIDS = 1 } ctlcu_plan_form;
-/* The form a plan kept and the replay times (ms) measured for both at its creation. */
+typedef enum { CTLCU_PLAN_CHOOSE = -1, CTLCU_PLAN_PERSISTENT = 0, CTLCU_PLAN_GRIDS = 1 } ctlcu_plan_form;
+/* The form a plan kept and the replay times (ms) measured for both at its
+ * creation (0 for a plan created in a given form). */
 CTLCU_API int ctlcu_plan_info(const ctlcu_plan* plan, int* form, float* ms_persistent, float* ms_grids);
+/* ctlcu_plan_create in a given form (CTLCU_PLAN_PERSISTENT or CTLCU_PLAN_GRIDS),
+ * without timing anything at creation; CTLCU_PLAN_CHOOSE is ctlcu_plan_create. */
+CTLCU_API int ctlcu_plan_create_form(ctlcu_ctx* ctx, const ctlcu_request* requests, uint32_t n_requests,
+                                     const ctlcu_settings* settings, int form, ctlcu_plan** plan);
 
 /* ---- several devices ---------------------------------------------------------------------- */
 

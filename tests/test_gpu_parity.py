@@ -333,7 +333,37 @@ def _uneven_requests(ctx, rng_seed=5):
 
 
 @pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_PAIRS], ids=["cells", "pairs"])
-def test_persistent_batch_matches_oracle_and_single_calls(ctx, kernel):
+def test_plan_forms_agree_with_single_calls(ctx, kernel):
+    """A plan's two forms -- one persistent launch over every request's warp patches,
+    and one grid launch per request on parallel graph branches -- give the same bits,
+    and those of single calls, within the oracle's bar."""
+    import torch
+    reqs, meta = _uneven_requests(ctx, rng_seed=21)
+    got = {}
+    for form in (L.PLAN_PERSISTENT, L.PLAN_GRIDS):
+        for _, _, out in reqs:
+            out.zero_()
+        plan = ctx.plan(reqs, Settings(kernel=kernel), form=form)
+        assert plan.info()["form"] == ("persistent" if form == L.PLAN_PERSISTENT else "grids")
+        plan.launch()
+        ctx.sync()
+        got[form] = [out.clone() for _, _, out in reqs]
+        plan.close()
+    for a, b in zip(got[L.PLAN_PERSISTENT], got[L.PLAN_GRIDS]):
+        assert torch.equal(a, b)
+    for out, (v, dP, _), (vol, vox, P, C, R) in zip(got[L.PLAN_GRIDS], reqs, meta):
+        single = ctx.project(v, P, C, R, Settings(kernel=kernel))
+        np.testing.assert_array_equal(out.cpu().numpy(), single)
+        want, _ = oracle.project_fp64(vol, (vox,) * 3, P, C, R)
+        assert rel_err(out.cpu().numpy(), want).max() <= TOL
+    with pytest.raises(L.CtlcuError):
+        ctx.plan(reqs, Settings(), form=7)
+    for v, _, _ in reqs:
+        v.release()
+
+
+@pytest.mark.parametrize("kernel", [L.KERNEL_CELLS, L.KERNEL_PAIRS], ids=["cells", "pairs"])
+def test_batch_matches_oracle_and_single_calls(ctx, kernel):
     reqs, meta = _uneven_requests(ctx)
     ctx.project_batch(reqs, Settings(kernel=kernel))
     ctx.sync()
