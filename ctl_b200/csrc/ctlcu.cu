@@ -968,7 +968,7 @@ int upload_batch(ctlcu_ctx* ctx, BatchPrep& bp, cudaStream_t st, bool pooled, Ba
     CU_TRY(ctx, alloc((void**)&bd.geom, sizeof(ViewGeom) * (size_t)bp.total_vm));
     CU_TRY(ctx, alloc((void**)&bd.setups, sizeof(BatchSetup) * n));
     CU_TRY(ctx, alloc((void**)&bd.reqs, sizeof(BatchReq) * n));
-    CU_TRY(ctx, alloc((void**)&bd.counter, sizeof(unsigned int) * kBatchCounters));
+    CU_TRY(ctx, alloc((void**)&bd.counter, sizeof(unsigned int)));
     for (size_t i = 0; i < n; ++i)
         bp.reqs[i].a.geom = bd.geom + bp.first_vm[i];
     CU_TRY(ctx, cudaMemcpyAsync(bd.setups, bp.setups.data(), sizeof(BatchSetup) * n, cudaMemcpyHostToDevice, st));
@@ -980,7 +980,7 @@ int enqueue_batch(ctlcu_ctx* ctx, const BatchPrep& bp, const BatchDevice& bd, co
                   cudaStream_t st)
 {
     const uint32_t n = (uint32_t)bp.reqs.size();
-    CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int) * kBatchCounters, st));
+    CU_TRY(ctx, cudaMemsetAsync(bd.counter, 0, sizeof(unsigned int), st));
     CU_TRY(ctx, launch_batch_setup(bd.setups, n, bp.total_vm, bd.geom, ctx->d_flags, st));
     int blocks = 0;
     CU_TRY(ctx, launch_batch(bd.reqs, n, bp.total_items, bp.mode, bp.acc, bp.shape, bd.counter, &blocks, st));

@@ -76,12 +76,6 @@ inline const char* shape_error(const LaunchShape& s)
 constexpr int kFlagSingular = 1;   // a projection matrix with singular / non-finite M
 constexpr int kFlagNonFinite = 2;  // a ray with non-finite entry/exit parameters
 
-#ifndef CTLCU_BATCH_DISPATCH
-#define CTLCU_BATCH_DISPATCH 0  // persistent batch kernel: 0 one queue of warp patches for all warps;
-                                // 2 one contiguous range of warp patches per SM, with stealing
-#endif
-// Counters a persistent batch launch may use (zeroed before it): one per SM range.
-constexpr int kBatchCounters = 1024;
 
 // Per (view, module) geometry, written by the FP64 setup kernel.
 struct ViewGeom {
@@ -251,8 +245,8 @@ cudaError_t launch_batch_setup(const BatchSetup* reqs, uint32_t n_reqs, uint32_t
 // Persistent launch (Mode::Cells or Mode::Pairs) over all work items of a
 // batch (total_items block tiles, each block / 32 warp patches, dealt out to
 // warps one patch at a time), every request with the launch shape `shape`
-// (block size and unroll); `counter` points to kBatchCounters counters that
-// must be zero at launch.  Returns the grid size in *blocks.
+// (block size and unroll); `counter` must be zero at launch.  Returns the
+// grid size in *blocks.
 cudaError_t launch_batch(const BatchReq* reqs, uint32_t n_reqs, uint32_t total_items, Mode mode, Accum acc,
                          const LaunchShape& shape, unsigned int* counter, int* blocks, cudaStream_t s);
 cudaError_t launch_setup(const double* pmats, uint32_t n_views, uint32_t n_modules, ViewGeom* geom,

@@ -743,65 +743,25 @@ __global__ void __maxnreg__(CTLCU_CELL_MAXREG) cells_kernel(const ProjectArgs a)
 // previous one (a warp's items only grow), and the request's launch arguments
 // are copied into the warp's own slot of shared memory only when the request
 // changes.
-#if CTLCU_BATCH_DISPATCH == 2
-// SM-local dispatch: the warp items are cut into n_ranges contiguous ranges, one
-// per SM, each with its own counter.  A warp takes items from the range of the
-// SM it runs on, so the SM's warps work on neighbouring patches, tiles and views
-// and share cells in its L1; once that range is empty it takes items from the
-// next range, and so on round the ranges until n_ranges of them in a row were
-// empty.  Counters only grow, so every item is taken exactly once; nothing waits.
-__device__ __forceinline__ uint32_t sm_local_next(unsigned int* counters, uint32_t n_ranges, uint32_t total,
-                                                  uint32_t& r)
-{
-    for (uint32_t empty = 0; empty < n_ranges; ++empty) {
-        const uint64_t lo = (uint64_t)r * total / n_ranges, hi = (uint64_t)(r + 1) * total / n_ranges;
-        const uint32_t k = atomicAdd(&counters[r], 1u);
-        if (lo + k < hi)
-            return (uint32_t)(lo + k);
-        r = (r + 1 == n_ranges) ? 0 : r + 1;
-    }
-    return 0xffffffffu;
-}
-#endif
 
 template <Mode M, Accum ACC, int U>
 __global__ void __maxnreg__(CTLCU_CELL_MAXREG)
     batch_cells_kernel(const BatchReq* __restrict__ reqs, uint32_t n_reqs, uint32_t total_warp_items,
-                       uint32_t wpb_shift, unsigned int* counter, uint32_t n_ranges)
+                       uint32_t wpb_shift, unsigned int* counter)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];  // one ProjectArgs per warp
     static_assert(sizeof(ProjectArgs) % 4 == 0, "word copy");
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     ProjectArgs& sa = reinterpret_cast<ProjectArgs*>(s_raw)[warp];
     uint32_t req = 0, loaded = 0xffffffffu;  // the same in every lane of the warp
-#if CTLCU_BATCH_DISPATCH == 2
-    uint32_t range = 0;
-    {
-        uint32_t smid;
-        asm("mov.u32 %0, %%smid;" : "=r"(smid));
-        range = smid % n_ranges;
-    }
-#else
-    (void)n_ranges;
-#endif
     for (;;) {
         uint32_t it = 0;
-#if CTLCU_BATCH_DISPATCH == 2
-        if (lane == 0)
-            it = sm_local_next(counter, n_ranges, total_warp_items, range);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it == 0xffffffffu)
-            return;
-#else
         if (lane == 0)
             it = atomicAdd(counter, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= total_warp_items)
             return;
-#endif
         const uint32_t item = it >> wpb_shift, w = it & ((1u << wpb_shift) - 1u);
-        if (item < reqs[req].first_item)
-            req = 0;  // a warp that moved on to an earlier range scans again from the start
         while (req + 1 < n_reqs && reqs[req + 1].first_item <= item)
             ++req;  // the last request with first_item <= item
         if (req != loaded) {
@@ -963,9 +923,8 @@ cudaError_t launch_batch_typed(const BatchReq* reqs, uint32_t n_reqs, uint32_t t
     if (grid > total)
         grid = total;
     *blocks = (int)grid;
-    const uint32_t n_ranges = (uint32_t)std::min<int>(std::max(sms, 1), kBatchCounters);
     batch_cells_kernel<M, ACC, U><<<(unsigned)grid, block, smem, s>>>(reqs, n_reqs, (uint32_t)warp_items, wpb_shift,
-                                                                      counter, n_ranges);
+                                                                      counter);
     return cudaGetLastError();
 }
 
