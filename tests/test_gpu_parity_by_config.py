@@ -13,7 +13,7 @@ ours.  Cases, at sizes the CPU checkers finish in seconds:
       trilinear cell loop with Kahan, FP64 and plain FP32 accumulation, the
       gather loop, the hardware texture filter, BF16 and F16 storage
   C4  one view of every one of the 64 uneven volumes, F32 and BF16, all in one
-      persistent batch
+      batch
   C5  two perturbed views of 256^2 on each of the 8 resident BF16 volumes, one
       batch
 
