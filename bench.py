@@ -960,12 +960,14 @@ def drr_measurements(ctx, args, sweep: bool = True) -> dict:
     kernel = {"auto": L.KERNEL_AUTO, "gather": L.KERNEL_GATHER, "cells": L.KERNEL_CELLS,
               "pairs": L.KERNEL_PAIRS}[args.kernel]
     settings = Settings(kernel=kernel)
-    # 2 streams and batches of at most 24 views: a batch's launches hold the SMs
-    # until it is done, so bounding its views bounds how long later requests wait behind it
-    # 24 GB of the 40 GB budget reserved for results up front (the volumes and their
-    # cells take 4.7 GB): no batch waits for the allocator to grow
-    server = DRRServer(ctx, vols, 256, 256, settings, streams=2, max_batch=256,
-                       budget_bytes=40 * 10**9, max_batch_views=24, reserve_bytes=24 * 10**9)
+    # 4 streams and batches of at most 12 views: a batch's launches hold the SMs until
+    # they are done, so bounding its views bounds how long later requests wait behind it
+    # (a sweep of 1-4 streams and 12-32 views gave this the highest capacity and the
+    # lowest p99 at 700-900 requests/s).  24 GB of the 40 GB budget are reserved for
+    # results up front (the volumes and their cells take 4.7 GB): no batch waits for the
+    # allocator to grow
+    server = DRRServer(ctx, vols, 256, 256, settings, streams=4, max_batch=256,
+                       budget_bytes=40 * 10**9, max_batch_views=12, reserve_bytes=24 * 10**9)
     base = W.c5_base_view()
     server.warm_up(typical_pmats=np.repeat(base[None], 8, axis=0) if kernel == L.KERNEL_AUTO else None)
     # capacity: all requests offered at once.  The first run of this size also grows the
@@ -1006,7 +1008,7 @@ def drr_measurements(ctx, args, sweep: bool = True) -> dict:
                             "samples_per_s_needed": samples / span_s,
                             "samples_per_s_at_capacity": samples / n_views * cap["throughput_views_s"]},
            "workload": "8 resident 256^3 BF16 volumes; Poisson 2000/s; 1-16 perturbed views of 256^2 @1.2 mm; "
-                       "40 GB budget (24 GB reserved for results); 2 streams, <= 24 views per batch",
+                       "40 GB budget (24 GB reserved for results); 4 streams, <= 12 views per batch",
            "launch_shapes": [ctx.tuned_settings(v, 1, 256, 256, settings).launch_shape() for v in vols]}
     for v in vols:
         v.release()
