@@ -127,11 +127,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _launched_by_torchrun() -> bool:
+    return "TORCHELASTIC_RUN_ID" in os.environ or int(os.environ.get("WORLD_SIZE", "1")) > 1
+
+
 def dist_setup(n_gpus):
+    """One process per GPU.  Under torchrun the NCCL group is made for any world
+    size, one rank included, so the barrier and the max over ranks take the same
+    NCCL path at every N."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if _launched_by_torchrun():
         import datetime
 
         import torch
@@ -142,8 +149,13 @@ def dist_setup(n_gpus):
     return world, rank, local
 
 
+def _dist_on() -> bool:
+    import torch.distributed as dist
+    return dist.is_available() and dist.is_initialized()
+
+
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
+    if not _dist_on():
         return x
     import torch
     import torch.distributed as dist
@@ -153,7 +165,7 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 def barrier(world):
-    if world > 1:
+    if _dist_on():
         import torch.distributed as dist
         dist.barrier()
 
@@ -404,7 +416,7 @@ def run_ours(args):
         print(json.dumps(line))
     volume.release()
     ctx.close()
-    if world > 1:
+    if _dist_on():
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
