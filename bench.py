@@ -1055,7 +1055,7 @@ def main():
     ap.add_argument("--unroll", type=int, default=0, choices=[0, 2, 4, 8])
     ap.add_argument("--views", type=int, default=N_VIEWS,
                     help="views per step (360 = the configuration; fewer = a small profiling case)")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-views", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -72,6 +72,7 @@ struct ctlcu_ctx {
     std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, Tuned> tuned;
     DenStaging den;  // pinned buffers for DEN file streaming, allocated on first use
     cudaStream_t copy_stream = nullptr;  // device-to-host copies that overlap projection
+    cudaStream_t aux_stream = nullptr;   // every other chunk of a projection into host memory
     // ctlcu_project_volume's resident copies of host volumes (ctlcu_set_volume_cache):
     // the volume's description and a hash of its whole content identify it
     struct Cached {
@@ -637,7 +638,8 @@ ctlcu_settings resolve_kernel(ctlcu_ctx* ctx, const VolumeEntry& v, const ctlcu_
 }
 
 int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s_in, const double* d_pm,
-                   uint32_t V, uint32_t M, uint32_t C, uint32_t R, float* d_out, cudaStream_t st)
+                   uint32_t V, uint32_t M, uint32_t C, uint32_t R, float* d_out, cudaStream_t st,
+                   bool st_ordered = false)
 {
     const ctlcu_settings eff = resolve_kernel(ctx, v, s_in, C, R, M);
     const ctlcu_settings* s = &eff;
@@ -647,9 +649,11 @@ int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s_in, c
     int r = volume_args(ctx, v, s, a, mode, dtype);
     if (r)
         return r;
-    r = order_after_staging(ctx, st);
-    if (r)
-        return r;
+    if (!st_ordered) {
+        r = order_after_staging(ctx, st);
+        if (r)
+            return r;
+    }
     job_args(a, s, V, M, C, R);
     ViewGeom* geom = nullptr;
     CU_TRY(ctx, cudaMallocAsync((void**)&geom, sizeof(ViewGeom) * (size_t)V * M, st));
@@ -662,6 +666,31 @@ int project_device(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s_in, c
     ctx->launches += 2;
     CU_TRY(ctx, cudaFreeAsync(geom, st));
     return CTLCU_OK;
+}
+
+// Views per chunk of a projection into host memory: five equal chunks, then
+// chunks of 4/47, 2/47 and 1/47 of the views (8, 4, 2, 1 parts of 47), so
+// that the copy that follows the last kernel is of about 2% of the output.  A
+// chunk's copy to the host takes a few percent of the time its views take to
+// project, so it stays hidden behind the next chunk, half as large.  Fewer
+// than 64 views: two chunks (3/4, 1/4); fewer than 8: one.
+std::vector<uint32_t> host_chunks(uint32_t V)
+{
+    if (V < 8)
+        return { V };
+    if (V < 64) {
+        const uint32_t a = (3 * V + 3) / 4;
+        return { a, V - a };
+    }
+    const uint32_t t4 = std::max(1u, 4 * V / 47), t2 = std::max(1u, 2 * V / 47), t1 = std::max(1u, V / 47);
+    const uint32_t lead = V - t4 - t2 - t1;
+    std::vector<uint32_t> n;
+    for (uint32_t i = 0; i < 5; ++i)
+        n.push_back(lead / 5 + (i < lead % 5 ? 1u : 0u));
+    n.push_back(t4);
+    n.push_back(t2);
+    n.push_back(t1);
+    return n;
 }
 
 int read_flags(ctlcu_ctx* ctx)
@@ -703,19 +732,30 @@ int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const d
         r = project_device(ctx, v, s, d_pm, V, M, C, R, d_out, st);
     } else {
         // Host output: the views go in chunks, and each chunk's copy to the host
-        // runs on the copy stream while the next chunk is projected.
+        // runs on the copy stream while the next chunk is projected.  Chunks
+        // alternate between two streams, so that a chunk's first blocks fill
+        // the SMs that the previous chunk's last blocks leave idle, and the
+        // last chunks are small, so that little copying follows the last kernel.
         if (!ctx->copy_stream)
             CU_TRY(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-        const uint32_t chunks = V >= 64 ? 8u : (V >= 8 ? 2u : 1u);
-        const uint32_t per = (V + chunks - 1) / chunks;
+        if (!ctx->aux_stream)
+            CU_TRY(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking));
+        // the second stream starts after the pmats upload and the volume staging on `st`
+        CU_TRY(ctx, cudaEventRecord(ctx->order, st));
+        CU_TRY(ctx, cudaStreamWaitEvent(ctx->aux_stream, ctx->order, 0));
+        const cudaStream_t lanes[2] = { st, ctx->aux_stream };
+        const std::vector<uint32_t> sizes = host_chunks(V);
         const size_t view_values = (size_t)M * R * C;
-        for (uint32_t first = 0; r == CTLCU_OK && first < V; first += per) {
-            const uint32_t n = std::min(per, V - first);
-            r = project_device(ctx, v, s, d_pm + (size_t)first * M * 12, n, M, C, R, d_out + first * view_values, st);
+        uint32_t first = 0;
+        for (size_t i = 0; r == CTLCU_OK && i < sizes.size(); first += sizes[i], ++i) {
+            const uint32_t n = sizes[i];
+            const cudaStream_t cs = lanes[i & 1];
+            r = project_device(ctx, v, s, d_pm + (size_t)first * M * 12, n, M, C, R, d_out + first * view_values, cs,
+                               true);
             cudaEvent_t done = nullptr;
             cudaError_t e = r ? cudaSuccess : cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
             if (!r && e == cudaSuccess)
-                e = cudaEventRecord(done, st);
+                e = cudaEventRecord(done, cs);
             if (!r && e == cudaSuccess)
                 e = cudaStreamWaitEvent(ctx->copy_stream, done, 0);
             if (!r && e == cudaSuccess)
@@ -726,15 +766,23 @@ int project_any(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, const d
             if (!r && e != cudaSuccess)
                 r = fail(ctx, CTLCU_ERR_CUDA, "copy of projections to the host failed: %s", cudaGetErrorString(e));
         }
-        // the device buffer is freed on `st`: order that after the last copy
-        cudaEvent_t copied = nullptr;
-        if (cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) == cudaSuccess) {
+        // the device buffers are freed on `st`: order that after the last copy
+        // and after everything on the second stream
+        cudaEvent_t copied = nullptr, aux_done = nullptr;
+        if (cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&aux_done, cudaEventDisableTiming) == cudaSuccess) {
             cudaEventRecord(copied, ctx->copy_stream);
+            cudaEventRecord(aux_done, ctx->aux_stream);
             cudaStreamWaitEvent(st, copied, 0);
-            cudaEventDestroy(copied);
+            cudaStreamWaitEvent(st, aux_done, 0);
         } else {
             cudaStreamSynchronize(ctx->copy_stream);
+            cudaStreamSynchronize(ctx->aux_stream);
         }
+        if (copied)
+            cudaEventDestroy(copied);
+        if (aux_done)
+            cudaEventDestroy(aux_done);
     }
     if (pm_tmp)
         cudaFreeAsync(pm_tmp, st);
@@ -1227,6 +1275,10 @@ int ctlcu_destroy(ctlcu_ctx* ctx)
         if (ctx->copy_stream) {
             cudaStreamSynchronize(ctx->copy_stream);
             cudaStreamDestroy(ctx->copy_stream);
+        }
+        if (ctx->aux_stream) {
+            cudaStreamSynchronize(ctx->aux_stream);
+            cudaStreamDestroy(ctx->aux_stream);
         }
         cudaStreamDestroy(ctx->stream);
     }

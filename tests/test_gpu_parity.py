@@ -127,6 +127,26 @@ def test_resident_device_and_host_paths_agree_bitwise(ctx):
     v.release()
 
 
+@pytest.mark.parametrize("n_views", [1, 7, 8, 9, 63, 64, 65, 90, 181])
+def test_host_output_chunks_cover_every_view_once(ctx, n_views):
+    """A projection into host memory goes in chunks over two streams (five equal
+    chunks and three smaller ones from 64 views up, two below, one below 8); every
+    view lands once, with the bits of the device-output call."""
+    import torch
+    from ctl_b200 import workloads as W
+    job = W.c1()
+    P = np.ascontiguousarray(np.concatenate([job.pmats, job.pmats, job.pmats])[:n_views])
+    v = ctx.volume(VoxelVolume(job.volume, job.voxel))
+    dev = ctx.project(v, torch.from_numpy(P).cuda(), job.channels, job.rows, Settings())
+    host = np.full((n_views, 1, job.rows, job.channels), np.nan, np.float32)
+    ctx.project(v, P, job.channels, job.rows, Settings(), out=host)
+    once = ctx.project_volume(VoxelVolume(job.volume, job.voxel), P, job.channels, job.rows, Settings())
+    want = dev.cpu().numpy()
+    np.testing.assert_array_equal(host, want)
+    np.testing.assert_array_equal(once, want)
+    v.release()
+
+
 def test_device_call_is_ordered_on_torchs_current_stream(ctx):
     """Without an explicit stream, a device-tensor call runs on torch's current
     stream (the default stream included), so a torch read-back that follows it
