@@ -368,7 +368,7 @@ def run_ours(args):
                     "loop": {L.KERNEL_CELLS: "cells", L.KERNEL_PAIRS: "pairs",
                              L.KERNEL_GATHER: "gather"}.get(loop, "auto"),
                     "launch_shape": shape, "views_of_rank0": [v0, v1]},
-            "vs_baseline_note": "no published number for this metric (BASELINE.md section 1)",
+            "vs_baseline_note": "the reference publishes no number for this metric",
             "samples_per_step": samples,
             "gsamples_per_s": samples * args.steps / (own_ms / 1e3) / 1e9,
             "e2e": {"value": e2e_value, "unit": "projections/s",
