@@ -143,3 +143,49 @@ def test_random_case_matches_oracle(ctx, seed):
         err = _max_rel(got, want)
         assert err <= 1e-4, (seed, k, err, {x: c[x] for x in c if x not in ("volume", "pmats")})
     h.release()
+
+
+def _batchable(seed: int) -> bool:
+    c = random_case(seed)
+    return c["interpolate"] and c["upsampling"] == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("batch", range(6))
+def test_random_batch_equals_single_calls(ctx, batch):
+    """Eight random cases (different volumes, storage types, detectors, modules and
+    view counts) in one batch, one settings for all: ctlcu_project_batch and a plan
+    in each form give every request the bits of its single call."""
+    import torch
+    from ctl_b200.projector import Settings, VoxelVolume
+    rng = np.random.default_rng(77 + batch)
+    seeds = [s for s in range(N_CASES) if _batchable(s)]
+    pick = [seeds[int(i)] for i in rng.choice(len(seeds), 8, replace=False)]
+    kernel = [L.KERNEL_CELLS, L.KERNEL_PAIRS][batch % 2]
+    s = Settings(rays_per_pixel=[int(rng.integers(1, 3)), int(rng.integers(1, 3))],
+                 ray_sampling=float(rng.uniform(0.15, 0.8)), kernel=kernel)
+    reqs, singles, handles = [], [], []
+    for seed in pick:
+        c = random_case(seed)
+        h = ctx.volume(VoxelVolume(c["volume"], c["voxel"], c["offset"]), c["storage"])
+        handles.append(h)
+        V, M = c["pmats"].shape[:2]
+        out = torch.full((V, M, c["rows"], c["channels"]), float("nan"), device="cuda")
+        reqs.append((h, torch.from_numpy(c["pmats"]).cuda(), out))
+        singles.append(ctx.project(h, c["pmats"], c["channels"], c["rows"], s))
+    ctx.project_batch(reqs, s)
+    ctx.sync()
+    for (_, _, out), want in zip(reqs, singles):
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+    for form in (L.PLAN_PERSISTENT, L.PLAN_GRIDS):
+        for _, _, out in reqs:
+            out.fill_(float("nan"))
+        plan = ctx.plan(reqs, s, form=form)
+        plan.launch()
+        ctx.sync()
+        for (_, _, out), want in zip(reqs, singles):
+            np.testing.assert_array_equal(out.cpu().numpy(), want)
+        plan.close()
+    del reqs
+    for h in handles:
+        h.release()
