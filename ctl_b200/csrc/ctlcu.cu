@@ -41,7 +41,6 @@ struct VolumeEntry {
     float* mean = nullptr;      // padded 1x1x1 mean volume (f = 0), float
     void* cells = nullptr;      // coefficient cells (CTLCU_KERNEL_CELLS), built on first use
     size_t cell_bytes = 0;
-    cudaTextureObject_t cell_tex = 0;  // linear float4 texture over `cells` (texture-fetch variant)
     uint32_t plan_refs = 0;     // plans that reference this volume (release is refused meanwhile)
     void* pairs = nullptr;      // x-pair array (CTLCU_KERNEL_PAIRS), built on first use
     size_t pair_bytes = 0;
@@ -322,9 +321,6 @@ void free_volume(ctlcu_ctx* ctx, VolumeEntry& v)
     if (v.mean)
         cudaFreeAsync(v.mean, ctx->stream);
     v.mean = nullptr;
-    if (v.cell_tex)
-        cudaDestroyTextureObject(v.cell_tex);
-    v.cell_tex = 0;
     if (v.cells) {
         if (v.pooled)
             cudaFreeAsync(v.cells, ctx->stream);
@@ -393,16 +389,6 @@ int ensure_cells(ctlcu_ctx* ctx, VolumeEntry& v)
     ctx->used += bytes;
     CU_TRY(ctx, launch_build_cells(v.data, n, v.desc.dtype, L, v.cells, ctx->stream));
     ++ctx->launches;
-    if (CTLCU_CELL_CACHE == 3) {
-        cudaResourceDesc rd = {};
-        rd.resType = cudaResourceTypeLinear;
-        rd.res.linear.devPtr = v.cells;
-        rd.res.linear.desc = cudaCreateChannelDesc<float4>();
-        rd.res.linear.sizeInBytes = bytes;
-        cudaTextureDesc td = {};
-        td.readMode = cudaReadModeElementType;
-        CU_TRY(ctx, cudaCreateTextureObject(&v.cell_tex, &rd, &td, nullptr));
-    }
     return CTLCU_OK;
 }
 
@@ -549,7 +535,6 @@ int volume_args(ctlcu_ctx* ctx, VolumeEntry& v, const ctlcu_settings* s, Project
             return r;
         mode = Mode::Cells;
         a.cells = v.cells;
-        a.cell_tex = v.cell_tex;
         const int n[3] = { (int)d.n[0], (int)d.n[1], (int)d.n[2] };
         const CellLayout L = cell_layout(n);
         a.csy = L.sy;

@@ -99,14 +99,6 @@ constexpr int kCellBytes = 32;
 // kMagicBits * (1 + sy + sz) = 0 mod 2^32, and the index of the cell whose
 // per-axis magic sums have bit patterns bx, by, bz is exactly
 // bx + by sy + bz sz in 32-bit arithmetic.
-//
-// With CTLCU_CELL_ZFAST the roles of x and z are swapped: z is the fastest
-// axis (stride 1), y has stride sy, x stride sz.  Warps are patches of
-// detector rows and channels; for scans about the z axis the rows run along
-// z, so a warp's cells then share cache lines.
-#ifndef CTLCU_CELL_ZFAST
-#define CTLCU_CELL_ZFAST 0
-#endif
 struct CellLayout {
     uint32_t cx, cy, cz;  // cells per axis
     uint32_t sy, sz;      // strides (cells) of y and of the slowest axis
@@ -120,13 +112,12 @@ inline CellLayout cell_layout(const int n[3])
     L.cx = (uint32_t)(n[0] + 2 * kPad - 1);
     L.cy = (uint32_t)(n[1] + 2 * kPad - 1);
     L.cz = (uint32_t)(n[2] + 2 * kPad - 1);
-    const uint32_t fast = CTLCU_CELL_ZFAST ? L.cz : L.cx, slow = CTLCU_CELL_ZFAST ? L.cx : L.cz;
-    L.sy = fast;
-    const uint32_t base = fast * L.cy;
+    L.sy = L.cx;
+    const uint32_t base = L.cx * L.cy;
     const uint32_t e = (1024u - ((1u + L.sy + base) & 1023u)) & 1023u;
     L.sz = base + e;
-    L.count = (uint64_t)L.sz * slow;
-    L.max_index = (slow - 1) * L.sz + (L.cy - 1) * L.sy + (fast - 1);
+    L.count = (uint64_t)L.sz * L.cz;
+    L.max_index = (L.cz - 1) * L.sz + (L.cy - 1) * L.sy + (L.cx - 1);
     return L;
 }
 
@@ -134,26 +125,8 @@ inline CellLayout cell_layout(const int n[3])
 __host__ __device__ __forceinline__ uint32_t cell_linear(uint32_t ix, uint32_t iy, uint32_t iz, uint32_t sy,
                                                          uint32_t sz)
 {
-#if CTLCU_CELL_ZFAST
-    return iz + iy * sy + ix * sz;
-#else
     return ix + iy * sy + iz * sz;
-#endif
 }
-
-#ifndef CTLCU_CELL_CACHE
-#define CTLCU_CELL_CACHE 2  // one-sample loop (CTLCU_CELL_PAIRED 0) only: 0: load every sample;
-                            // 1: load on cell change (branch); 2: predicated load; 3: texture fetch on change
-#endif
-
-#ifndef CTLCU_CELL_PAIRED
-#define CTLCU_CELL_PAIRED 1  // 1: the cell loop forms two consecutive samples' positions per packed f32x2
-                             // operation (1.6% faster at 256^3 -> 512^2, the same bits); 0: one sample at a time
-#endif
-
-#ifndef CTLCU_CELL_PREFETCH
-#define CTLCU_CELL_PREFETCH 0  // samples ahead to prefetch the cell into L1 (0 = off)
-#endif
 
 // x-pair array: for every padded voxel (x < ext_x - 1, y, z) the float2
 // (mid, diff) = ((v[x] + v[x+1]) / 2, v[x+1] - v[x]), computed in FP64.  A
@@ -198,7 +171,6 @@ struct ProjectArgs {
     double corner[3];         // low corner of that grid (mm)
     double increment;         // step length (mm)
     const void* cells;        // Mode::Cells: coefficient cells, x fastest
-    cudaTextureObject_t cell_tex;  // the same cells as a linear float4 texture (0 if absent)
     uint32_t csy, csz;        // cell strides (cells per row, per slice)
     uint32_t cmax;            // last valid cell index
     uint32_t vm_group;        // view groups per chunk of the block order

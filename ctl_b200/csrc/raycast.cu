@@ -300,100 +300,16 @@ __device__ __forceinline__ CellFrame cell_frame(const Ray& r)
     return f;
 }
 
-// One sample from the coefficient cells at step kk (both lanes of kk hold k).
-// Per axis: v' = (base - I) + k step; t = v' + m rounds to the cell index (its
-// bits minus kMagicBits, see CellFrame); h = v' - (t - m) is the offset from
-// the cell centre in [-1/2, 1/2].  x and y go through packed f32x2 arithmetic.
-// A sample that lands exactly between two cells may take either of them; both
-// give the same interpolated value.  The cell index is clamped to the array as
-// a guard; the loop bounds already keep every sample inside it.
+// The coefficients of the cell a ray is in, reloaded only when its cell
+// changes (consecutive samples of a ray often share a cell).
 struct CellCache {
     uint32_t idx = 0xffffffffu;  // cell whose coefficients c0..c7 hold
     float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f;
 };
 
-#if CTLCU_CELL_PREFETCH > 0
-// Cell index of the sample at step kk (the cell layout makes the magic
-// offsets cancel, see CellLayout), clamped to the array.
-__device__ __forceinline__ uint32_t cell_index(float2 kk, const CellFrame& fr, float2 dxy, float dz,
-                                               uint32_t sy, uint32_t sz, uint32_t cmax)
-{
-    const float2 txy = __fadd2_rn(__ffma2_rn(kk, dxy, fr.bxy), fr.mxy);
-    const float tz = __fadd_rn(fmaf(kk.x, dz, fr.bz), fr.mz);
-    const uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
-    return min(idx, cmax);
-}
-#endif
-
-#if !CTLCU_CELL_PAIRED
-// (the one-sample loop; the paired loop below uses cell_sample_pair)
-__device__ __forceinline__ float cell_sample(cudaTextureObject_t ctex, const char* __restrict__ cells, float2 kk,
-                                             const CellFrame& fr, float2 dxy, float dz, uint32_t sy, uint32_t sz,
-                                             uint32_t cmax, CellCache& cc)
-{
-    const float2 none2 = make_float2(-1.0f, -1.0f);
-    const float2 vxy = __ffma2_rn(kk, dxy, fr.bxy);
-    const float vz = fmaf(kk.x, dz, fr.bz);
-    const float2 txy = __fadd2_rn(vxy, fr.mxy);
-    const float tz = __fadd_rn(vz, fr.mz);
-    const float2 fxy = __ffma2_rn(fr.mxy, none2, txy);  // t - m, exact
-    const float fz = __fsub_rn(tz, fr.mz);
-    const float2 hxy = __ffma2_rn(fxy, none2, vxy);
-    const float hz = fmaf(fz, -1.0f, vz);
-    uint32_t idx = cell_linear(__float_as_uint(txy.x), __float_as_uint(txy.y), __float_as_uint(tz), sy, sz);
-    idx = min(idx, cmax);
-    // consecutive samples of a ray often fall in the same cell: reload only on a change
-#if CTLCU_CELL_CACHE == 0
-    {
-        const char* p = cells + (size_t)idx * kCellBytes;
-        asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                     : "=f"(cc.c0), "=f"(cc.c1), "=f"(cc.c2), "=f"(cc.c3), "=f"(cc.c4), "=f"(cc.c5),
-                       "=f"(cc.c6), "=f"(cc.c7)
-                     : "l"(p));
-    }
-#elif CTLCU_CELL_CACHE == 3
-    if (idx != cc.idx) {
-        // through the texture pipeline: two float4 texels per cell
-        const float4 lo = tex1Dfetch<float4>(ctex, (int)(2 * idx));
-        const float4 hi = tex1Dfetch<float4>(ctex, (int)(2 * idx + 1));
-        cc.c0 = lo.x; cc.c1 = lo.y; cc.c2 = lo.z; cc.c3 = lo.w;
-        cc.c4 = hi.x; cc.c5 = hi.y; cc.c6 = hi.z; cc.c7 = hi.w;
-        cc.idx = idx;
-    }
-#elif CTLCU_CELL_CACHE == 2
-    {
-        // predicated load: registers keep the cached cell when the index is unchanged
-        const char* p = cells + (size_t)idx * kCellBytes;
-        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %8, %9;\n\t"
-                     "@p ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%10];\n\t}"
-                     : "+f"(cc.c0), "+f"(cc.c1), "+f"(cc.c2), "+f"(cc.c3), "+f"(cc.c4), "+f"(cc.c5),
-                       "+f"(cc.c6), "+f"(cc.c7)
-                     : "r"(idx), "r"(cc.idx), "l"(p));
-        cc.idx = idx;
-    }
-#else
-    if (idx != cc.idx) {
-        const char* p = cells + (size_t)idx * kCellBytes;
-        asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                     : "=f"(cc.c0), "=f"(cc.c1), "=f"(cc.c2), "=f"(cc.c3), "=f"(cc.c4), "=f"(cc.c5),
-                       "=f"(cc.c6), "=f"(cc.c7)
-                     : "l"(p));
-        cc.idx = idx;
-    }
-#endif
-    // (C0, Cz), (Cx, Cxz), (Cy, Cyz), (Cxy, Cxyz)
-    const float2 hx2 = make_float2(hxy.x, hxy.x);
-    const float2 ea = __ffma2_rn(hx2, make_float2(cc.c2, cc.c3), make_float2(cc.c0, cc.c1));
-    const float2 eb = __ffma2_rn(hx2, make_float2(cc.c6, cc.c7), make_float2(cc.c4, cc.c5));
-    const float2 g = __ffma2_rn(make_float2(hxy.y, hxy.y), eb, ea);
-    return fmaf(hz, g.y, g.x);
-}
-
-#endif
-
-#if CTLCU_CELL_PAIRED
 // The interpolant of the cached cell at offsets (hx, hy, hz) from its centre,
-// loading the cell first if `idx` differs from the cached one (see cell_sample).
+// loading the cell first if `idx` differs from the cached one: a predicated
+// 32-byte load, so the registers keep the cached cell when it does not.
 __device__ __forceinline__ float cell_eval(const char* __restrict__ cells, uint32_t idx, float hx, float hy,
                                            float hz, CellCache& cc)
 {
@@ -413,11 +329,14 @@ __device__ __forceinline__ float cell_eval(const char* __restrict__ cells, uint3
     return fmaf(hz, g.y, g.x);
 }
 
-// Two consecutive samples (steps k and k + 1, the lanes of kk) of cell_sample
-// at once: each packed f32x2 operation holds one axis of both samples, so the
-// position, rounding and offset arithmetic of the z axis shares the packed
-// instructions of x and y.  Per sample the operations and their rounding are
-// those of cell_sample, so the values are identical.
+// Two consecutive samples of a ray (steps k and k + 1, the lanes of kk) from
+// the coefficient cells.  Per axis: v' = (base - I) + k step; t = v' + m rounds
+// to the cell index (its bits minus kMagicBits, see CellFrame); h = v' - (t - m)
+// is the offset from the cell centre in [-1/2, 1/2].  Each packed f32x2
+// operation holds one axis of both samples.  A sample that lands exactly
+// between two cells may take either of them; both give the same interpolated
+// value.  The cell index is clamped to the array as a guard; the loop bounds
+// already keep every sample inside it.
 __device__ __forceinline__ float2 cell_sample_pair(const char* __restrict__ cells, float2 kk, const CellFrame& fr,
                                                    float2 dx2, float2 dy2, float2 dz2, uint32_t sy, uint32_t sz,
                                                    uint32_t cmax, CellCache& cc)
@@ -440,14 +359,12 @@ __device__ __forceinline__ float2 cell_sample_pair(const char* __restrict__ cell
     const float f1 = cell_eval(cells, i1, hx.y, hy.y, hz.y, cc);
     return make_float2(f0, f1);
 }
-#endif
 
 // Sample loop over the coefficient cells, U samples per partial sum (FP32)
 // handed to the accumulator.
 template <Accum ACC, int U>
 __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, Accumulator<ACC>& acc)
 {
-#if CTLCU_CELL_PAIRED
     const char* __restrict__ cells = static_cast<const char*>(a.cells);
     const CellFrame fr = cell_frame(r);
     const float2 dx2 = make_float2((float)r.step[0], (float)r.step[0]);
@@ -482,47 +399,6 @@ __device__ __forceinline__ void march_cells(const ProjectArgs& a, const Ray& r, 
         if (k < r.n)
             acc.add(cell_sample_pair(cells, kk, fr, dx2, dy2, dz2, sy, sz, cmax, cc).x);
     }
-#else
-    const char* __restrict__ cells = static_cast<const char*>(a.cells);
-    const CellFrame fr = cell_frame(r);
-    const float2 dxy = make_float2((float)r.step[0], (float)r.step[1]);
-    const float dz = (float)r.step[2];
-    const uint32_t sy = a.csy, sz = a.csz, cmax = a.cmax;
-    const float2 one2 = make_float2(1.0f, 1.0f);
-    float2 kk = make_float2(0.0f, 0.0f);
-    CellCache cc;
-#if CTLCU_CELL_PREFETCH > 0
-    __shared__ float prefetch_sink[kMaxBlock];
-    const uint32_t prefetch_slot = (uint32_t)__cvta_generic_to_shared(&prefetch_sink[threadIdx.x]);
-#endif
-    int k = 0;
-    for (; k + U <= r.n; k += U) {
-        float part = 0.0f;
-#if CTLCU_CELL_PREFETCH > 0
-        {
-            // pull the cell of sample k + PREFETCH into L1 without waiting for it:
-            // an asynchronous 4-byte copy into a scratch shared word that is never read
-            const float ahead = (float)CTLCU_CELL_PREFETCH;
-            const uint32_t pi = cell_index(__fadd2_rn(kk, make_float2(ahead, ahead)), fr, dxy, dz, sy, sz, cmax);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(prefetch_slot),
-                         "l"(cells + (size_t)pi * kCellBytes));
-        }
-#endif
-#pragma unroll
-        for (int j = 0; j < U; ++j) {
-            part += cell_sample(a.cell_tex, cells, kk, fr, dxy, dz, sy, sz, cmax, cc);
-            kk = __fadd2_rn(kk, one2);
-        }
-        acc.add(part);
-    }
-    for (; k < r.n; ++k) {
-        acc.add(cell_sample(a.cell_tex, cells, kk, fr, dxy, dz, sy, sz, cmax, cc));
-        kk = __fadd2_rn(kk, one2);
-    }
-#if CTLCU_CELL_PREFETCH > 0
-    asm volatile("cp.async.wait_all;" ::: "memory");
-#endif
-#endif
 }
 
 // x-pair entries of the current cell: rows (y, z), (y+1, z), (y, z+1), (y+1, z+1).
@@ -532,7 +408,7 @@ struct PairCache {
 };
 
 // One sample from the x-pair array: the same cell index and centre offsets as
-// cell_sample, four 8-byte entries loaded only when the cell changes, x by
+// cell_sample_pair, four 8-byte entries loaded only when the cell changes, x by
 // mid + hx diff, then y and z linearly.
 __device__ __forceinline__ float pair_sample(const char* __restrict__ pairs, float2 kk, const CellFrame& fr,
                                              float2 dxy, float dz, uint32_t sy, uint32_t sz, uint32_t pmax,
